@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 `tdse` propagation (one JSON line on rank 0).
+
+Workload (default): the plain 2e helium CI case -- total L = 0..3, blocks of
+3983/4411/4702/4904 states (18000 complex128 coefficients), 61.8M dense
+real64 dipole elements (495 MB), velocity gauge, sin^2 pulse 390 nm
+(3.179 eV), 5e14 W/cm^2, 8 cycles, dt = 0.1 with the reference's semantics
+(field frozen at t+dt per step, renormalisation after every step), started
+from the CI ground state.  The H0 spectrum and dipole blocks are seeded
+synthetic data with that layout (the structure programs that produce real
+ones are not part of this library).
+
+A step is one pulse advanced by one RKF78 step (13 right-hand sides).
+  value    pulse-steps/s with the state resident in HBM (mpc_advance);
+  e2e      the same through the C ABI entry point mpc_propagate on pinned
+           host buffers, one call per step: each step copies the state in
+           and the state plus the step's population/field/norm out;
+  roofline the dipole-streaming kernel: algorithmic bytes per launch (each
+           dipole element once, 8 B, plus the stage vector) over its mean
+           launch time (CUDA events on the library's stream), against the
+           measured HBM copy bandwidth;
+  cpu_baseline / --impl reference: the reference's own src/tdse/tdse.cpp
+           (built under oracle/_ref with OpenBLAS on all host cores) timed on
+           a bounded number of steps of the same workload.
+Multi-GPU (torchrun): every rank propagates its own pulse replica (pulses are
+independent; no collective on the data path), value = all ranks' steps over
+the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mp-citdse_b200"))
+
+METRIC = "pulse-steps/s, batched vs plain GPU at ≤1e-9 pop. error; adjoint grads/s"
+UNIT = "pulse-steps/s"
+
+WORKLOADS = {
+    "he2e": dict(kind="2e", n=(3983, 4411, 4702, 4904), gauge="v", w_eV=3.179, Io=5e14,
+                 cycles=8, dt=0.1,
+                 desc="2e He CI-like, L=0..3, 18000 states, velocity gauge, sin^2 390 nm "
+                      "5e14 W/cm^2 8 cycles, dt=0.1, reference semantics"),
+    "h1e": dict(kind="1e", n=(298,) * 6, gauge="l", w_eV=1.5498, Io=1e14, cycles=10, dt=0.1,
+                desc="1e H-like, l=0..5, 298 states/l, length gauge, sin^2 800 nm 1e14 W/cm^2 "
+                     "10 cycles, dt=0.1, reference semantics"),
+}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_system(w):
+    from mpc_tdse.systems import helium_like_2e, hydrogen_like_1e
+
+    if w["kind"] == "2e":
+        return helium_like_2e(w["n"], gauge=w["gauge"], seed=0)
+    return hydrogen_like_1e(w["n"][0], len(w["n"]) - 1, gauge=w["gauge"], seed=0)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev_uuid):
+        self.uuid = dev_uuid
+        self.p = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.TemporaryFile(mode="w+")
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                   "-lms", "200"]
+            if self.uuid:
+                cmd += ["-i", self.uuid]
+            self.p = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 8:
+                continue
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_rate(system, w, nsteps, threads):
+    """The reference's own propagation loop (oracle/_ref) on host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    from oracle import Reference
+
+    if not Reference.available():
+        return None
+    ref = Reference()
+    ref.use_openblas(threads)
+    x0 = np.zeros(system.ntot, complex)
+    x0[0] = 1.0
+    with tempfile.TemporaryDirectory() as d:
+        t = time.perf_counter()
+        ref.propagate(system.n, system.eig, system.dip, w["gauge"], "sine", w["Io"], w["w_eV"],
+                      w["cycles"], 0.0, w["dt"], nsteps, x0, os.path.join(d, "he"))
+        el = time.perf_counter() - t
+    return nsteps / el, el
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    w = WORKLOADS[args.workload]
+    system = make_system(w)
+    threads = os.cpu_count() or 1
+    # each bench step is one call of the reference's propV/propL over 10 pulse
+    # steps (its loop needs >= 10); the run stops early once ~120 s are spent
+    chunk = 10
+    rates, spent, done = [], 0.0, 0
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_rate(system, w, chunk, threads)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "oracle/_ref/libref_tdse.so not built (needs the reference tree)"}))
+            return
+        if i >= args.warmup:
+            rates.append(r[1])
+            done += chunk
+        spent += r[1]
+        if spent > 120.0 and done > 0:
+            break
+    tot = sum(rates)
+    value = done / tot
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * tot / done,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": w["desc"], "states": list(w["n"])},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{done} pulse-steps in calls of {chunk} (reference "
+                                   "tdse::propV/propL, odeint RKF78 stand-in, OpenBLAS "
+                                   f"{threads} threads)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="he2e", choices=list(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="full", choices=["full", "kernel"],
+                    help="kernel: only warm-up + timed steps of the workload (a small case for "
+                         "profilers); no JSON line")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+
+    import mpc_tdse
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    w = WORKLOADS[args.workload]
+    system = make_system(w)
+    S = int((system.n[:-1].astype(np.int64) * system.n[1:]).sum())
+    ntot = system.ntot
+    ctx = mpc_tdse.Context.from_system(system, device=local)
+    Io, wau = mpc_tdse.to_au(w["Io"], w["w_eV"])
+    tau = mpc_tdse.period(wau, w["cycles"])
+    pulse = mpc_tdse.pulse_setup("sine", w["gauge"], Io, wau, 0.0, w["cycles"], tau)
+    dt = w["dt"]
+    x0 = np.zeros(ntot, complex)
+    x0[0] = 1.0
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    # ---- value: device-resident state -------------------------------------
+    ctx.state_set(x0)
+    ctx.advance(pulse, 0.0, dt, args.warmup)
+    ctx.sync()
+    t_start = args.warmup * dt
+    props = torch.cuda.get_device_properties(local)
+    uuid = getattr(props, "uuid", None)
+    sampler = ClockSampler(f"GPU-{uuid}" if uuid else None)
+    barrier()
+    launches0 = ctx.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler.start()
+    time.sleep(0.25)
+    e0.record(stream)
+    ctx.advance(pulse, t_start, dt, args.steps)
+    e1.record(stream)
+    ctx.sync()
+    clocks = sampler.stop()
+    launches = ctx.launches - launches0
+    ms = e0.elapsed_time(e1)
+    if args.mode == "kernel":
+        ctx.close()
+        return
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps / (ms / 1000.0)
+
+    # ---- roofline of the dipole-streaming kernel (separate profiled pass) --
+    prof_steps = min(args.steps, 50)
+    ctx.profile(True)
+    ctx.advance(pulse, t_start, dt, prof_steps)
+    rhs_ms, rhs_n = ctx.profile_read("rhs_stream")
+    cmb_ms, cmb_n = ctx.profile_read("combine")
+    ren_ms, ren_n = ctx.profile_read("renorm")
+    ctx.profile(False)
+    bytes_per_launch = 8 * S + 16 * ntot
+    avg_s = rhs_ms / rhs_n / 1000.0
+    peak, peak_src = load_peaks()
+    achieved = bytes_per_launch / avg_s / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "rhs_stream_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(args.workload)
+    tot_k = rhs_ms + cmb_ms + ren_ms
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "kernel": "k_rhs_stream", "peak_source": f"{peak_src} hbm_gbs",
+                "bytes_per_launch": bytes_per_launch, "avg_launch_us": avg_s * 1e6,
+                "share": {"rhs_stream": rhs_ms / tot_k, "combine": cmb_ms / tot_k,
+                          "renorm": ren_ms / tot_k}}
+
+    # ---- e2e: C ABI on pinned host buffers, one call per step ---------------
+    ct = torch.zeros(2 * ntot, dtype=torch.float64, pin_memory=True).numpy()
+    pop = torch.zeros(2, dtype=torch.float64, pin_memory=True).numpy()
+    fld = torch.zeros(1, dtype=torch.float64, pin_memory=True).numpy()
+    nrm = torch.zeros(1, dtype=torch.float64, pin_memory=True).numpy()
+    ct[:] = x0.view(np.float64)
+    e2e_steps = args.steps
+    for i in range(args.warmup):
+        ctx.propagate_into(pulse, i * dt, dt, 1, ct, pop, fld, nrm)
+    barrier()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for i in range(e2e_steps):
+        ctx.propagate_into(pulse, t_start + i * dt, dt, 1, ct, pop, fld, nrm)
+    e1.record(stream)
+    ctx.sync()
+    wall = time.perf_counter() - t0
+    e2e_ms = max(e0.elapsed_time(e1), 1000.0 * wall)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * e2e_steps / (e2e_ms / 1000.0), "unit": UNIT,
+           "h2d_bytes_per_step": 16 * ntot + 8,
+           "d2h_bytes_per_step": 16 * ntot + 16 + 8 + 8}
+
+    # ---- CPU baseline (rank 0, N=1) -----------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        r = cpu_reference_rate(system, w, 10 if w["kind"] == "2e" else 200, threads)
+        if r is not None:
+            cpu = {"value": r[0], "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{10 if w['kind'] == '2e' else 200} pulse-steps of this workload "
+                             f"in {r[1]:.1f} s (reference tdse::propV/propL, odeint RKF78 "
+                             "stand-in, OpenBLAS)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w["desc"], "states": list(w["n"]), "dipole_elements": S,
+                       "dipole_bytes": 8 * S, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2: the dipole blocks (%.0f MB) stream "
+                             "through every right-hand side" % (8 * S / 1e6)
+                             if 8 * S > 126e6 else "dipole blocks fit in L2"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clocks,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,152 @@
+/*
+ * mpc_tdse.h -- C ABI of the B200 implementation of MP-CITDSE's `tdse`
+ * propagation (libmpc_tdse.so).
+ *
+ * Everything is plain C: ints, doubles, host or device pointers and sizes.
+ * Every function returns MPC_OK (0) or a negative MPC_ERR_* code; the text of
+ * the last error on the calling thread is available from mpc_last_error().
+ *
+ * Array conventions are the reference's (citations are paths inside the
+ * MP-CITDSE source tree):
+ *   - state_sz[L], L = 0..L_max: states kept per angular-momentum block, as
+ *     Propagator_Settings.states_in_l (src/tdse/td_read.cpp:17-26);
+ *   - eig: the per-block eigenenergies concatenated (tdrd::readEnergies,
+ *     src/tdse/td_read.cpp:50-86);
+ *   - dip: the dipole blocks back to back, block L row-major
+ *     [state_sz[L] x state_sz[L+1]] (tdrd::readDipoles,
+ *     src/tdse/td_read.cpp:88-120);
+ *   - a state (ct) is interleaved complex128: 2*sum(state_sz) doubles
+ *     (state_type, src/tdse/tdse.cpp:3).
+ *
+ * A context owns its device copies, its CUDA stream and its work buffers.
+ * Contexts are not thread-safe: use one per host thread.
+ */
+#ifndef MPC_TDSE_H_
+#define MPC_TDSE_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPC_OK 0
+#define MPC_ERR_ARG (-1)      /* invalid argument                          */
+#define MPC_ERR_CUDA (-2)     /* a CUDA runtime call failed                */
+#define MPC_ERR_DEVICE (-3)   /* a kernel reported a failure (status word) */
+#define MPC_ERR_NOMEM (-4)    /* device allocation failed                  */
+#define MPC_ERR_UNSTABLE (-5) /* dt outside the RKF78 stability interval   */
+
+/* Field shapes: pulse::sineEE, sineAA, sineAE, sineEA and gauss
+ * (src/tdse/pulse.cpp:34-97). */
+#define MPC_FIELD_SINE_EE 0
+#define MPC_FIELD_SINE_AA 1
+#define MPC_FIELD_SINE_AE 2
+#define MPC_FIELD_SINE_EA 3
+#define MPC_FIELD_GAUSS 4
+
+/* pulse::params (src/tdse/include/pulse.hpp:20-26) plus the field function
+ * the reference's main binds to it (src/tdse/tdse_main.cpp:166-192). */
+typedef struct mpc_pulse {
+  int kind; /* MPC_FIELD_* */
+  double Eo, w, cepd, a, b;
+} mpc_pulse;
+
+typedef struct mpc_ctx mpc_ctx;
+
+/* Version of this ABI (major*10000 + minor*100 + patch). */
+int mpc_version(void);
+
+/* Copies the last error message of the calling thread into buf. */
+int mpc_last_error(char *buf, size_t len);
+
+/* Pulse set-up in atomic units, as pulse::sineESetup / sineASetup /
+ * gaussESetup / gaussASetup (src/tdse/pulse.cpp:10-32,41-47,69-75):
+ * shape 0 = sin^2 envelope, 1 = Gaussian; gauge 'l' gives an E-defined pulse
+ * (sineEE / gauss), 'v' an A-defined one (sineAA / gauss). */
+int mpc_pulse_setup(int shape, char gauge, double Io_au, double w_au, double cepd, int cycles,
+                    double tau, mpc_pulse *out);
+
+/* pulse::toAU (src/tdse/pulse.cpp:3-6), pulse::period (:8). */
+int mpc_to_au(double Io_Wcm2, double w_eV, double *Io_au, double *w_au);
+double mpc_period(double w_au, int cycles);
+
+/* The field function bound to `p` at time t (src/tdse/pulse.cpp:34-97). */
+double mpc_field(const mpc_pulse *p, double t);
+
+/* Creates a context on CUDA device `device` holding H0 and the dipole
+ * blocks.  Replaces the MatVecV / MatVecL set-up in tdse::propV / propL
+ * (src/tdse/tdse.cpp:159-169): the blocks are copied to HBM once and stay
+ * resident.  gauge: 'l' (MatVecL) or 'v' (MatVecV). */
+int mpc_ctx_create(int L_max, const int *state_sz, const double *eig, const double *dip,
+                   char gauge, int device, mpc_ctx **out);
+int mpc_ctx_destroy(mpc_ctx *ctx);
+
+/* Total number of states sum(state_sz). */
+int mpc_ctx_size(const mpc_ctx *ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that record
+ * events or order their own work after the library's. */
+int mpc_ctx_stream(const mpc_ctx *ctx, void **stream);
+
+/* One right-hand-side evaluation dxdt = f(x) at field value F:
+ * MatVecV::operator() / MatVecL::operator() (src/tdse/tdse.cpp:14-73,
+ * :85-143).  Host buffers of 2*size doubles. */
+int mpc_rhs(mpc_ctx *ctx, double F, const double *x, double *dxdt);
+
+/* One rkf.do_step(sys, x, t, dt) with the field frozen at F
+ * (src/tdse/tdse.cpp:190): 13 stages, 8th-order solution, no
+ * renormalisation.  x: host, in/out. */
+int mpc_rk78_step(mpc_ctx *ctx, double F, double dt, double *x);
+
+/* The propagation loop of tdse::propV / tdse::propL
+ * (src/tdse/tdse.cpp:186-215): for each of `steps` steps, F = field(t+dt)
+ * frozen for the step, one RKF78 step, t += dt, ct /= ||ct||_2.
+ * ct: host, in/out.  Optional host outputs (NULL to skip):
+ *   pop_out[steps+1]   |ct[pop_index]|^2 at t0 and after every step
+ *                      (the reference's _pop<n><l>.dat column);
+ *   field_out[steps]   the field used by each step (_field.dat column);
+ *   norm_out[steps]    ||ct|| before each renormalisation (norm drift).
+ * Returns MPC_ERR_UNSTABLE if dt*(max|E| + max|F|*||D||) lies outside the
+ * RKF78 imaginary-axis stability interval. */
+int mpc_propagate(mpc_ctx *ctx, const mpc_pulse *pulse, double t0, double dt, int steps,
+                  int pop_index, double *ct, double *pop_out, double *field_out,
+                  double *norm_out);
+
+/* Device-resident form of mpc_propagate: the state stays in the context.
+ * mpc_state_set / mpc_state_get copy it in / out (host buffers);
+ * mpc_advance runs the loop on the resident state without host copies
+ * (history outputs stay on the device and can be fetched with
+ * mpc_history_get). */
+int mpc_state_set(mpc_ctx *ctx, const double *ct);
+int mpc_state_get(mpc_ctx *ctx, double *ct);
+int mpc_advance(mpc_ctx *ctx, const mpc_pulse *pulse, double t0, double dt, int steps,
+                int pop_index);
+int mpc_history_get(mpc_ctx *ctx, int steps, double *pop_out, double *field_out,
+                    double *norm_out);
+
+/* Kernel timing (profiling aid).  While enabled, CUDA events on the
+ * context's stream bracket every launch of each kernel kind:
+ *   MPC_KERNEL_RHS_STREAM (0)  the dipole-block streaming pass,
+ *   MPC_KERNEL_COMBINE (1)     the per-stage epilogue,
+ *   MPC_KERNEL_RENORM (2)      the per-step renormalisation.
+ * mpc_profile_read returns the summed device milliseconds and the number of
+ * launches of one kind since the last read (and resets that kind). */
+#define MPC_KERNEL_RHS_STREAM 0
+#define MPC_KERNEL_COMBINE 1
+#define MPC_KERNEL_RENORM 2
+int mpc_profile_enable(mpc_ctx *ctx, int on);
+int mpc_profile_read(mpc_ctx *ctx, int kind, double *total_ms, long long *launches);
+
+/* Number of kernel launches the library issued on this context since it was
+ * created (all kinds). */
+long long mpc_launch_count(const mpc_ctx *ctx);
+
+/* Waits for the context's stream and returns any kernel-reported failure
+ * (MPC_ERR_DEVICE) or CUDA error. */
+int mpc_sync(mpc_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,204 @@
+// rhs_stream.cuh -- the dipole-coupling pass of one right-hand-side
+// evaluation, streaming every dipole block through shared memory once.
+//
+// Replaces the 4 strided cblas_dgemv calls per dipole block of
+// MatVecV/MatVecL::operator() (src/tdse/tdse.cpp:28-68, :99-139), which read
+// each block four times (Re/Im x D/D^T).  Here each element D[r][c] of block
+// L is read once from HBM and used twice:
+//   row partial  P_row[r] += D[r][c] * y_{L+1}[c]   (D_L y_{L+1} -> block L)
+//   col partial  P_col[c] += D[r][c] * y_L[r]       (D_L^T y_L   -> block L+1)
+// with y complex and D real, 4 DFMA per element.
+//
+// Layout: one persistent CTA per SM.  Warp 8 is the producer: one lane
+// issues 2-D TMA loads of 16x256 tiles into a kStages-deep shared-memory ring
+// (full/empty mbarriers).  Warps 0-7 consume: warp w takes rows 2w and 2w+1
+// of each tile; lane l holds the 8 columns {64j + 2l, 64j + 2l + 1}, j<4, of
+// the current strip.
+//   - Row partials are complete for the strip after a 6-shuffle
+//     reduce-scatter across the warp and are stored to RP[strip][row].
+//   - Column partials accumulate in registers while the CTA walks down a
+//     strip; when the strip (or the CTA's range) ends, the 8 warps' partials
+//     are summed in shared memory (warp order 0..7) and stored as one slot
+//     CP[slot][0..255].
+// Every output is written by exactly one thread in a fixed order, so repeated
+// runs give identical bits.
+#pragma once
+#include <cuda.h>
+
+#include "dev_util.cuh"
+#include "plan.h"
+
+namespace mpc {
+
+struct TmapSet {
+  CUtensorMap m[kMaxBlocks];
+};
+
+struct StreamArgs {
+  const double2* y;       // stage input, ntot complex
+  double2* RP;            // row partials
+  double2* CP;            // column partial slots, kStripW complex each
+  const int* cta_slot0;   // first CP slot of each CTA
+  unsigned* status;
+  Geometry g;
+};
+
+__device__ __forceinline__ double2 ld_y(const double2* y, int idx) {
+  return __ldg(y + idx);
+}
+
+__global__ void __launch_bounds__(kStreamThreads, 1)
+    k_rhs_stream(const __grid_constant__ StreamArgs a, const __grid_constant__ TmapSet tm) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  double* tiles = reinterpret_cast<double*>(smem);
+  double2* red = reinterpret_cast<double2*>(smem + kStages * kTileBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kTileBytes + kRedBytes);
+  uint64_t* empty = full + kStages;
+
+  const Geometry& g = a.g;
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int t_begin = (int)((long long)g.ntiles * blockIdx.x / gridDim.x);
+  const int t_end = (int)((long long)g.ntiles * (blockIdx.x + 1) / gridDim.x);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (t_begin >= t_end) return;
+
+  if (warp == kConsumerWarps) {
+    // ---------------- producer ----------------
+    if (lane != 0) return;
+    int issued = 0;
+    for (int t = t_begin; t < t_end; ++t, ++issued) {
+      const int stage = issued % kStages;
+      const int round = issued / kStages;
+      if (round > 0 && !mbar_wait_bounded(&empty[stage], (round - 1) & 1, a.status)) break;
+      int b, s, rt;
+      decode_tile(g, t, b, s, rt);
+      mbar_arrive_expect_tx(&full[stage], kTileBytes);
+      tma_load_2d(tiles + stage * (kTileR * kStripW), &tm.m[b], &full[stage], s * kStripW,
+                  rt * kTileR);
+    }
+    // Do not leave while a load is in flight: wait until every issued tile
+    // was released by the consumers, or, if they gave up, until it landed.
+    for (int i = (issued > kStages ? issued - kStages : 0); i < issued; ++i) {
+      const int stage = i % kStages;
+      const int round = i / kStages;
+      if (!mbar_wait_bounded(&empty[stage], round & 1, a.status))
+        mbar_wait_bounded(&full[stage], round & 1, a.status);
+    }
+    return;
+  }
+
+  // ---------------- consumers ----------------
+  double2 ycol[8];
+  double2 cacc[8];
+  int cur_b = -1, cur_s = -1;
+  int slot = a.cta_slot0[blockIdx.x] - 1;
+  const int ctid = threadIdx.x;  // 0..255 among consumers
+
+  auto flush_cols = [&](int b) {
+    // warp partials -> shared, then a fixed-order sum over warps
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      red[warp * kStripW + 64 * j + 2 * lane] = cacc[2 * j];
+      red[warp * kStripW + 64 * j + 2 * lane + 1] = cacc[2 * j + 1];
+    }
+    named_bar_sync(1, kConsumerWarps * 32);
+    double2 acc = red[ctid];
+#pragma unroll
+    for (int w = 1; w < kConsumerWarps; ++w) {
+      const double2 v = red[w * kStripW + ctid];
+      acc.x += v.x;
+      acc.y += v.y;
+    }
+    a.CP[(long long)slot * kStripW + ctid] = acc;
+    named_bar_sync(1, kConsumerWarps * 32);
+    (void)b;
+  };
+
+  // After a timed-out wait the warp keeps walking its tiles without reading
+  // shared memory, so that every consumer warp still reaches each named
+  // barrier; the raised status makes the host discard the result.
+  bool dead = false;
+  int it = 0;
+  for (int t = t_begin; t < t_end; ++t, ++it) {
+    int b, s, rt;
+    decode_tile(g, t, b, s, rt);
+    const BlockGeom& bg = g.blk[b];
+    if (b != cur_b || s != cur_s) {
+      if (cur_b >= 0) flush_cols(cur_b);
+      ++slot;
+      cur_b = b;
+      cur_s = s;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int c = s * kStripW + 64 * j + 2 * lane + e;
+          ycol[2 * j + e] = (c < bg.ncol) ? ld_y(a.y, bg.col_off + c) : make_double2(0.0, 0.0);
+          cacc[2 * j + e] = make_double2(0.0, 0.0);
+        }
+      }
+    }
+    const int r0 = rt * kTileR + 2 * warp;
+    const double2 yr0 = (r0 < bg.nrow) ? ld_y(a.y, bg.row_off + r0) : make_double2(0.0, 0.0);
+    const double2 yr1 =
+        (r0 + 1 < bg.nrow) ? ld_y(a.y, bg.row_off + r0 + 1) : make_double2(0.0, 0.0);
+
+    const int stage = it % kStages;
+    const int round = it / kStages;
+    if (!dead && !mbar_wait_bounded(&full[stage], round & 1, a.status)) dead = true;
+    const double* T = tiles + stage * (kTileR * kStripW);
+    const double* T0 = T + (2 * warp) * kStripW + 2 * lane;
+    const double* T1 = T0 + kStripW;
+    double2 ra = make_double2(0.0, 0.0), rb = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const double2 d0 = dead ? make_double2(0.0, 0.0) : *reinterpret_cast<const double2*>(T0 + 64 * j);
+      const double2 d1 = dead ? make_double2(0.0, 0.0) : *reinterpret_cast<const double2*>(T1 + 64 * j);
+      const double2 c0 = ycol[2 * j], c1 = ycol[2 * j + 1];
+      ra.x = fma(d0.x, c0.x, ra.x); ra.x = fma(d0.y, c1.x, ra.x);
+      ra.y = fma(d0.x, c0.y, ra.y); ra.y = fma(d0.y, c1.y, ra.y);
+      rb.x = fma(d1.x, c0.x, rb.x); rb.x = fma(d1.y, c1.x, rb.x);
+      rb.y = fma(d1.x, c0.y, rb.y); rb.y = fma(d1.y, c1.y, rb.y);
+      double2& q0 = cacc[2 * j];
+      double2& q1 = cacc[2 * j + 1];
+      q0.x = fma(d0.x, yr0.x, q0.x); q0.x = fma(d1.x, yr1.x, q0.x);
+      q0.y = fma(d0.x, yr0.y, q0.y); q0.y = fma(d1.x, yr1.y, q0.y);
+      q1.x = fma(d0.y, yr0.x, q1.x); q1.x = fma(d1.y, yr1.x, q1.x);
+      q1.y = fma(d0.y, yr0.y, q1.y); q1.y = fma(d1.y, yr1.y, q1.y);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[stage]);
+
+    // reduce-scatter of (ra.x, ra.y, rb.x, rb.y) over the 32 lanes:
+    // lane 0 -> ra.x, lane 8 -> ra.y, lane 16 -> rb.x, lane 24 -> rb.y
+    const bool hi16 = (lane & 16) != 0;
+    const double s0 = hi16 ? ra.x : rb.x, s1 = hi16 ? ra.y : rb.y;
+    const double k0 = hi16 ? rb.x : ra.x, k1 = hi16 ? rb.y : ra.y;
+    const double w0 = k0 + __shfl_xor_sync(0xffffffffu, s0, 16);
+    const double w1 = k1 + __shfl_xor_sync(0xffffffffu, s1, 16);
+    const bool hi8 = (lane & 8) != 0;
+    double z = (hi8 ? w1 : w0) + __shfl_xor_sync(0xffffffffu, hi8 ? w0 : w1, 8);
+    z += __shfl_xor_sync(0xffffffffu, z, 4);
+    z += __shfl_xor_sync(0xffffffffu, z, 2);
+    z += __shfl_xor_sync(0xffffffffu, z, 1);
+    if ((lane & 7) == 0) {
+      const int r = r0 + (hi16 ? 1 : 0);
+      if (r < bg.nrow) {
+        double* rp = reinterpret_cast<double*>(a.RP + bg.rp_off + (long long)s * bg.nrow + r);
+        rp[hi8 ? 1 : 0] = z;
+      }
+    }
+  }
+  if (cur_b >= 0) flush_cols(cur_b);
+}
+
+}  // namespace mpc

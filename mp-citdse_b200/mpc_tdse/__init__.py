@@ -1,0 +1,254 @@
+"""Python front end of libmpc_tdse.so (the C ABI in include/mpc_tdse.h).
+
+Mirrors the reference's in-process interface for the propagation path:
+
+* :class:`Context` holds what ``tdse::propV`` / ``tdse::propL`` receive --
+  ``state_sz``, the per-block energies ``eig`` and the dipole blocks
+  (src/tdse/include/tdse.hpp:66-101) -- resident on the GPU;
+* :meth:`Context.rhs` is ``MatVecV/MatVecL::operator()``
+  (src/tdse/tdse.cpp:14-73, :85-143);
+* :meth:`Context.rk78_step` is one ``rkf.do_step`` (src/tdse/tdse.cpp:190);
+* :meth:`Context.propagate` is the loop of ``propV``/``propL``
+  (src/tdse/tdse.cpp:186-215), returning the coefficient vector and the
+  per-step population / field / pre-renormalisation norm;
+* :func:`pulse_setup`, :func:`to_au`, :func:`period`, :func:`field` are
+  ``pulse::*Setup``, ``toAU``, ``period`` and the field functions
+  (src/tdse/pulse.cpp).
+
+All compute runs in the CUDA library; there is no CPU fallback.  Importing
+works without a GPU (the library loads), but creating a context needs one.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .systems import System  # noqa: F401
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libmpc_tdse.so")
+HEADER_PATH = os.path.join(os.path.dirname(os.path.dirname(_HERE)), "include", "mpc_tdse.h")
+
+MPC_OK = 0
+ERRORS = {-1: "MPC_ERR_ARG", -2: "MPC_ERR_CUDA", -3: "MPC_ERR_DEVICE", -4: "MPC_ERR_NOMEM",
+          -5: "MPC_ERR_UNSTABLE"}
+FIELD = {"sineEE": 0, "sineAA": 1, "sineAE": 2, "sineEA": 3, "gauss": 4}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class MpcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Pulse(C.Structure):
+    """``pulse::params`` plus the field function bound to it."""
+    _fields_ = [("kind", C.c_int), ("Eo", C.c_double), ("w", C.c_double),
+                ("cepd", C.c_double), ("a", C.c_double), ("b", C.c_double)]
+
+    def as_array(self):
+        return np.array([self.Eo, self.w, self.cepd, self.a, self.b])
+
+
+_lib = None
+
+
+def lib():
+    """Loads libmpc_tdse.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} not built; run __graft_entry__.build() "
+                          "(python -c 'import __graft_entry__ as g; g.build()')")
+    L = C.CDLL(LIB_PATH)
+    L.mpc_version.restype = C.c_int
+    L.mpc_last_error.argtypes = [C.c_char_p, C.c_size_t]
+    L.mpc_to_au.argtypes = [C.c_double, C.c_double, _dp, _dp]
+    L.mpc_period.restype = C.c_double
+    L.mpc_period.argtypes = [C.c_double, C.c_int]
+    L.mpc_pulse_setup.argtypes = [C.c_int, C.c_char, C.c_double, C.c_double, C.c_double,
+                                  C.c_int, C.c_double, C.POINTER(Pulse)]
+    L.mpc_field.restype = C.c_double
+    L.mpc_field.argtypes = [C.POINTER(Pulse), C.c_double]
+    L.mpc_ctx_create.argtypes = [C.c_int, _ip, _dp, _dp, C.c_char, C.c_int, C.POINTER(C.c_void_p)]
+    L.mpc_ctx_destroy.argtypes = [C.c_void_p]
+    L.mpc_ctx_size.argtypes = [C.c_void_p]
+    L.mpc_ctx_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    L.mpc_rhs.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
+    L.mpc_rk78_step.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp]
+    L.mpc_propagate.argtypes = [C.c_void_p, C.POINTER(Pulse), C.c_double, C.c_double, C.c_int,
+                                C.c_int, _dp, _dp, _dp, _dp]
+    L.mpc_state_set.argtypes = [C.c_void_p, _dp]
+    L.mpc_state_get.argtypes = [C.c_void_p, _dp]
+    L.mpc_advance.argtypes = [C.c_void_p, C.POINTER(Pulse), C.c_double, C.c_double, C.c_int,
+                              C.c_int]
+    L.mpc_history_get.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
+    L.mpc_sync.argtypes = [C.c_void_p]
+    L.mpc_profile_enable.argtypes = [C.c_void_p, C.c_int]
+    L.mpc_profile_read.argtypes = [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_longlong)]
+    L.mpc_launch_count.restype = C.c_longlong
+    L.mpc_launch_count.argtypes = [C.c_void_p]
+    _lib = L
+    return L
+
+
+def last_error():
+    buf = C.create_string_buffer(1024)
+    lib().mpc_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def _check(rc):
+    if rc != MPC_OK:
+        raise MpcError(rc, last_error())
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _state(x):
+    x = np.ascontiguousarray(x)
+    if np.iscomplexobj(x):
+        return np.ascontiguousarray(x, dtype=np.complex128).view(np.float64).copy()
+    return np.ascontiguousarray(x, dtype=np.float64).copy()
+
+
+def to_au(Io_Wcm2, w_eV):
+    a, b = C.c_double(), C.c_double()
+    _check(lib().mpc_to_au(Io_Wcm2, w_eV, C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+def period(w_au, cycles):
+    return lib().mpc_period(w_au, int(cycles))
+
+
+def pulse_setup(shape, gauge, Io_au, w_au, cepd, cycles, tau=0.0):
+    p = Pulse()
+    shp = {"sine": 0, "gaussian": 1, 0: 0, 1: 1}[shape]
+    _check(lib().mpc_pulse_setup(shp, gauge.encode(), Io_au, w_au, cepd, int(cycles), tau,
+                                 C.byref(p)))
+    return p
+
+
+def field(p, t):
+    return lib().mpc_field(C.byref(p), t)
+
+
+class Context:
+    """A system resident on one GPU (``mpc_ctx``)."""
+
+    def __init__(self, state_sz, eig, dip, gauge, device=0):
+        L = lib()
+        self.n = np.ascontiguousarray(state_sz, dtype=np.int32)
+        self.gauge = gauge
+        eig = np.ascontiguousarray(eig, dtype=np.float64)
+        dip = np.ascontiguousarray(dip, dtype=np.float64)
+        h = C.c_void_p()
+        _check(L.mpc_ctx_create(len(self.n) - 1, self.n.ctypes.data_as(_ip), _ptr(eig), _ptr(dip),
+                                gauge.encode(), int(device), C.byref(h)))
+        self._h = h
+        self.size = int(self.n.sum())
+
+    @classmethod
+    def from_system(cls, s, device=0):
+        return cls(s.n, s.eig, s.dip, s.gauge, device)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mpc_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def stream(self):
+        s = C.c_void_p()
+        _check(lib().mpc_ctx_stream(self._h, C.byref(s)))
+        return s.value
+
+    def rhs(self, F, x):
+        xf = _state(x)
+        out = np.empty_like(xf)
+        _check(lib().mpc_rhs(self._h, float(F), _ptr(xf), _ptr(out)))
+        return out.view(np.complex128)
+
+    def rk78_step(self, F, dt, x):
+        xf = _state(x)
+        _check(lib().mpc_rk78_step(self._h, float(F), float(dt), _ptr(xf)))
+        return xf.view(np.complex128)
+
+    def propagate(self, pulse, t0, dt, steps, x, pop_index=0, history=True):
+        """Returns (ct, pop[steps+1], field[steps], norm[steps]) (history optional)."""
+        xf = _state(x)
+        pop = np.empty(steps + 1) if history else None
+        fld = np.empty(max(steps, 1)) if history else None
+        nrm = np.empty(max(steps, 1)) if history else None
+        _check(lib().mpc_propagate(self._h, C.byref(pulse), float(t0), float(dt), int(steps),
+                                   int(pop_index), _ptr(xf), _ptr(pop), _ptr(fld), _ptr(nrm)))
+        ct = xf.view(np.complex128)
+        if not history:
+            return ct
+        return ct, pop, fld[:steps], nrm[:steps]
+
+    def propagate_into(self, pulse, t0, dt, steps, ct, pop=None, fld=None, nrm=None,
+                       pop_index=0):
+        """mpc_propagate on caller-owned float64 buffers (e.g. pinned host
+        memory), in place and without copies: ct [2*size], pop [steps+1],
+        fld [steps], nrm [steps]."""
+        _check(lib().mpc_propagate(self._h, C.byref(pulse), float(t0), float(dt), int(steps),
+                                   int(pop_index), _ptr(ct), _ptr(pop), _ptr(fld), _ptr(nrm)))
+
+    # device-resident form
+    def state_set(self, x):
+        self._xbuf = _state(x)
+        _check(lib().mpc_state_set(self._h, _ptr(self._xbuf)))
+
+    def state_get(self):
+        out = np.empty(2 * self.size)
+        _check(lib().mpc_state_get(self._h, _ptr(out)))
+        return out.view(np.complex128)
+
+    def advance(self, pulse, t0, dt, steps, pop_index=0):
+        _check(lib().mpc_advance(self._h, C.byref(pulse), float(t0), float(dt), int(steps),
+                                 int(pop_index)))
+
+    def history(self, steps):
+        pop, fld, nrm = np.empty(steps + 1), np.empty(max(steps, 1)), np.empty(max(steps, 1))
+        _check(lib().mpc_history_get(self._h, int(steps), _ptr(pop), _ptr(fld), _ptr(nrm)))
+        return pop, fld[:steps], nrm[:steps]
+
+    def sync(self):
+        _check(lib().mpc_sync(self._h))
+
+    KERNELS = {"rhs_stream": 0, "combine": 1, "renorm": 2}
+
+    def profile(self, on=True):
+        _check(lib().mpc_profile_enable(self._h, int(bool(on))))
+
+    def profile_read(self, kind):
+        ms, n = C.c_double(), C.c_longlong()
+        _check(lib().mpc_profile_read(self._h, self.KERNELS.get(kind, kind), C.byref(ms),
+                                      C.byref(n)))
+        return ms.value, n.value
+
+    @property
+    def launches(self):
+        return int(lib().mpc_launch_count(self._h))
