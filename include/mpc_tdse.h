@@ -142,6 +142,33 @@ int mpc_profile_read(mpc_ctx *ctx, int kind, double *total_ms, long long *launch
  * created (all kinds). */
 long long mpc_launch_count(const mpc_ctx *ctx);
 
+/* Right-hand side without any allocation.  No counterpart in the reference
+ * (it has no GPU path).
+ *
+ * For callers that cannot allocate device memory: a host framework whose
+ * caching allocator owns the device (a raw cudaMalloc can fail or fragment
+ * its pool), a plugin inside a simulation code that forbids allocation after
+ * start-up, a time-critical loop that cannot afford cudaMalloc/cudaFree and
+ * their implicit synchronisation.  Computes dxdt = f(x) at field F -- the
+ * same result as mpc_rhs -- on caller-owned DEVICE buffers of the current
+ * CUDA device: d_eig [sum(state_sz)], d_dip (blocks back to back, block L
+ * row-major [state_sz[L] x state_sz[L+1]]), d_x and d_dxdt [2*sum(state_sz)]
+ * doubles.  state_sz is a host array.  Runs asynchronously on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream).
+ *
+ * Its scratch is a static device array of MPC_NOALLOC_SCRATCH_BYTES (16 MiB)
+ * that every GPU loading the library holds until the process exits.  Systems
+ * needing more -- 16 B x (sum over dipole blocks of ceil(n_{L+1}/256) x n_L
+ * + 256 per column-partial slot) -- or more than 256 column strips are
+ * rejected with MPC_ERR_ARG.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture begins.  All calls share the array and it keeps the
+ * last call's contents: calls whose kernels overlap on the GPU race, so
+ * serialise them.  No cudaMalloc, cudaFree or host heap allocation. */
+#define MPC_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int mpc_rhs_noalloc(int L_max, const int *state_sz, const double *d_eig, const double *d_dip,
+                    char gauge, double F, const double *d_x, double *d_dxdt, void *stream);
+
 /* Waits for the context's stream and returns any kernel-reported failure
  * (MPC_ERR_DEVICE) or CUDA error. */
 int mpc_sync(mpc_ctx *ctx);

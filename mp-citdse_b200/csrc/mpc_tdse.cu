@@ -35,6 +35,9 @@ static int fail(int code, const char* fmt, ...) {
   return code;
 }
 
+// error reporting for the other translation units of the library
+int mpc_internal_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+
 #define CK(call)                                                                         \
   do {                                                                                   \
     cudaError_t e_ = (call);                                                             \
