@@ -4,6 +4,8 @@
 // k_stage_combine: for every state i (block L, local row r)
 //   Q = sum_strips RP_L[strip][r]                  (D_L y_{L+1}, if L < L_max)
 //   P = sum_slots  CP[slot][r mod 256]             (D_{L-1}^T y_{L-1}, if L > 0)
+//   (4 lanes per state, each summing every 4th strip / slot, then a fixed
+//   xor-shuffle tree: the order is fixed, so results repeat bit for bit)
 //   k_s[i] per gauge, in the reference's order of operations
 //   (src/tdse/tdse.cpp:14-73 velocity, :85-143 length):
 //     length:   Im: ((-e*Re y) + (-F)*P.re) + (-F)*Q.re
@@ -49,19 +51,24 @@ __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a,
 __global__ void __launch_bounds__(kCombineThreads)
     k_stage_combine(const __grid_constant__ CombineArgs a) {
   const Geometry& g = a.g;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double nsq = 0.0;
-  if (i < g.ntot) {
-    int L = 0;
+  // kCombineLanes consecutive threads share one coefficient: they split its
+  // partial sums (strip s and slot s handled by lane s mod kCombineLanes) and
+  // reduce them with a fixed shuffle tree; lane 0 finishes the coefficient.
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = gt / kCombineLanes;
+  const int q = gt % kCombineLanes;
+  const bool valid = i < g.ntot;
+  int L = 0, r = 0;
+  double2 Q = make_double2(0.0, 0.0), P = make_double2(0.0, 0.0);
+  if (valid) {
     while (L + 1 < g.nstate_blk && i >= g.state_off[L + 1]) ++L;
-    const int r = i - g.state_off[L];
-    double2 Q = make_double2(0.0, 0.0), P = make_double2(0.0, 0.0);
+    r = i - g.state_off[L];
     if (L < g.nblk) {
       const BlockGeom& b = g.blk[L];
       const double2* rp = a.RP + b.rp_off + r;
-      Q = rp[0];
-      for (int s = 1; s < b.nstrips; ++s) {
-        const double2 v = rp[(long long)s * b.nrow];
+#pragma unroll 4
+      for (int s = q; s < b.nstrips; s += kCombineLanes) {
+        const double2 v = rp[s * (long long)b.nrow];
         Q.x = dadd(Q.x, v.x);
         Q.y = dadd(Q.y, v.y);
       }
@@ -70,14 +77,23 @@ __global__ void __launch_bounds__(kCombineThreads)
       const BlockGeom& b = g.blk[L - 1];
       const int gs = b.strip0 + r / kStripW;
       const int c = r % kStripW;
-      const int s0 = a.strip_slot0[gs], s1 = a.strip_slot0[gs + 1];
-      P = a.CP[(long long)s0 * kStripW + c];
-      for (int sl = s0 + 1; sl < s1; ++sl) {
+      const int s1 = a.strip_slot0[gs + 1];
+      for (int sl = a.strip_slot0[gs] + q; sl < s1; sl += kCombineLanes) {
         const double2 v = a.CP[(long long)sl * kStripW + c];
         P.x = dadd(P.x, v.x);
         P.y = dadd(P.y, v.y);
       }
     }
+  }
+#pragma unroll
+  for (int o = 1; o < kCombineLanes; o <<= 1) {
+    Q.x = dadd(Q.x, __shfl_xor_sync(0xffffffffu, Q.x, o));
+    Q.y = dadd(Q.y, __shfl_xor_sync(0xffffffffu, Q.y, o));
+    P.x = dadd(P.x, __shfl_xor_sync(0xffffffffu, P.x, o));
+    P.y = dadd(P.y, __shfl_xor_sync(0xffffffffu, P.y, o));
+  }
+  double nsq = 0.0;
+  if (valid && q == 0) {
     const double F = a.Ftab[a.step];
     const double e = a.eps[i];
     const double2 y = a.y[i];
@@ -92,14 +108,22 @@ __global__ void __launch_bounds__(kCombineThreads)
     }
     const long long n = g.ntot;
     a.k[a.stage * n + i] = make_double2(kre, kim);
+    // load every earlier k_j first, then sum left to right
+    double2 kj[kNumStages];
+#pragma unroll
+    for (int m = 0; m < kNumStages; ++m)
+      if (m < a.ncoef) {
+        const int j = a.coef_j[m];
+        kj[m] = (j == a.stage) ? make_double2(kre, kim) : a.k[j * n + i];
+      }
     double2 acc = a.x[i];
-    for (int m = 0; m < a.ncoef; ++m) {
-      const int j = a.coef_j[m];
-      const double c = a.coef[m];
-      const double2 kj = (j == a.stage) ? make_double2(kre, kim) : a.k[j * n + i];
-      acc.x = dadd(acc.x, dmul(c, kj.x));
-      acc.y = dadd(acc.y, dmul(c, kj.y));
-    }
+#pragma unroll
+    for (int m = 0; m < kNumStages; ++m)
+      if (m < a.ncoef) {
+        const double c = a.coef[m];
+        acc.x = dadd(acc.x, dmul(c, kj[m].x));
+        acc.y = dadd(acc.y, dmul(c, kj[m].y));
+      }
     a.out[i] = acc;
     nsq = dadd(dmul(acc.x, acc.x), dmul(acc.y, acc.y));
   }

@@ -181,7 +181,7 @@ void plan_geometry(mpc_ctx* c, const int* n, int L_max, std::vector<int>& cta_sl
   }
   strip_slot0[g.nstrips] = slot;
   nslots = slot;
-  c->combine_grid = (g.ntot + kCombineThreads - 1) / kCombineThreads;
+  c->combine_grid = (g.ntot * kCombineLanes + kCombineThreads - 1) / kCombineThreads;
 }
 
 int ensure_hist(mpc_ctx* c, int steps) {
@@ -485,7 +485,7 @@ int mpc_ctx_create(int L_max, const int* state_sz, const double* eig, const doub
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(MPC_ERR_CUDA, "cudaStreamCreate failed"));
   if ((rc = dalloc(c, &c->d_eps, g.ntot)) || (rc = dalloc(c, &c->d_D, d_total)) ||
-      (rc = dalloc(c, &c->d_x, g.ntot)) || (rc = dalloc(c, &c->d_y, g.ntot)) ||
+      (rc = dalloc(c, &c->d_x, g.ntot + kVecPad)) || (rc = dalloc(c, &c->d_y, g.ntot + kVecPad)) ||
       (rc = dalloc(c, &c->d_k, (size_t)kNumStages * g.ntot)) ||
       (rc = dalloc(c, &c->d_RP, rp_total)) ||
       (rc = dalloc(c, &c->d_CP, (size_t)nslots * kStripW)) ||
@@ -501,6 +501,8 @@ int mpc_ctx_create(int L_max, const int* state_sz, const double* eig, const doub
       up(c->d_cta_slot0, cta_slot0.data(), sizeof(int) * cta_slot0.size()) != cudaSuccess ||
       up(c->d_strip_slot0, strip_slot0.data(), sizeof(int) * strip_slot0.size()) != cudaSuccess ||
       cudaMemset(c->d_status, 0, sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(c->d_x, 0, sizeof(double2) * (g.ntot + kVecPad)) != cudaSuccess ||
+      cudaMemset(c->d_y, 0, sizeof(double2) * (g.ntot + kVecPad)) != cudaSuccess ||
       cudaMemset(c->d_D, 0, sizeof(double) * d_total) != cudaSuccess)
     return bail(fail(MPC_ERR_CUDA, "upload failed"));
   const double* src = dip;

@@ -19,14 +19,17 @@ namespace mpc {
 constexpr int kMaxBlocks = 16;      // angular-momentum blocks L = 0..15
 constexpr int kStripW = 256;        // tile width (columns, doubles)
 constexpr int kTileR = 16;          // tile height (rows)
-constexpr int kStages = 5;          // TMA ring depth
+constexpr int kStages = 6;          // TMA ring depth
 constexpr int kConsumerWarps = 8;   // warps that compute; one more issues TMA
 constexpr int kStreamThreads = (kConsumerWarps + 1) * 32;
 constexpr int kTileBytes = kTileR * kStripW * 8;
+constexpr int kYRowBytes = kTileR * 16;          // the tile's stage-vector rows
 constexpr int kRedBytes = kConsumerWarps * kStripW * 16;
-constexpr int kStreamSmem = kStages * kTileBytes + kRedBytes + 2 * kStages * 8;
+constexpr int kStreamSmem = kStages * (kTileBytes + kYRowBytes) + kRedBytes + 2 * kStages * 8;
+constexpr int kVecPad = kTileR;     // zeroed tail of every stage vector (row bulk copies)
 constexpr int kNumStages = 13;      // RKF78 stages
 constexpr int kCombineThreads = 256;
+constexpr int kCombineLanes = 4;    // threads cooperating on one coefficient
 
 struct BlockGeom {
   int nrow, ncol;        // n_L, n_{L+1}

@@ -10,8 +10,10 @@
 // with y complex and D real, 4 DFMA per element.
 //
 // Layout: one persistent CTA per SM.  Warp 8 is the producer: one lane
-// issues 2-D TMA loads of 16x256 tiles into a kStages-deep shared-memory ring
-// (full/empty mbarriers).  Warps 0-7 consume: warp w takes rows 2w and 2w+1
+// issues 2-D TMA loads of 16x256 tiles (with an L2 evict-first hint: the
+// blocks are streamed once per pass) plus a 1-D bulk copy of the tile's 16
+// stage-vector rows into a kStages-deep shared-memory ring (full/empty
+// mbarriers).  Warps 0-7 consume: warp w takes rows 2w and 2w+1
 // of each tile; lane l holds the 8 columns {64j + 2l, 64j + 2l + 1}, j<4, of
 // the current strip.
 //   - Row partials are complete for the strip after a 6-shuffle
@@ -51,8 +53,10 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
     k_rhs_stream(const __grid_constant__ StreamArgs a, const __grid_constant__ TmapSet tm) {
   extern __shared__ __align__(1024) unsigned char smem[];
   double* tiles = reinterpret_cast<double*>(smem);
-  double2* red = reinterpret_cast<double2*>(smem + kStages * kTileBytes);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kTileBytes + kRedBytes);
+  double2* yrows = reinterpret_cast<double2*>(smem + kStages * kTileBytes);
+  double2* red = reinterpret_cast<double2*>(smem + kStages * (kTileBytes + kYRowBytes));
+  uint64_t* full =
+      reinterpret_cast<uint64_t*>(smem + kStages * (kTileBytes + kYRowBytes) + kRedBytes);
   uint64_t* empty = full + kStages;
 
   const Geometry& g = a.g;
@@ -74,6 +78,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   if (warp == kConsumerWarps) {
     // ---------------- producer ----------------
     if (lane != 0) return;
+    const uint64_t policy = make_evict_first_policy();
     int issued = 0;
     for (int t = t_begin; t < t_end; ++t, ++issued) {
       const int stage = issued % kStages;
@@ -81,9 +86,13 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
       if (round > 0 && !mbar_wait_bounded(&empty[stage], (round - 1) & 1, a.status)) break;
       int b, s, rt;
       decode_tile(g, t, b, s, rt);
-      mbar_arrive_expect_tx(&full[stage], kTileBytes);
-      tma_load_2d(tiles + stage * (kTileR * kStripW), &tm.m[b], &full[stage], s * kStripW,
-                  rt * kTileR);
+      mbar_arrive_expect_tx(&full[stage], kTileBytes + kYRowBytes);
+      tma_load_2d_hint(tiles + stage * (kTileR * kStripW), &tm.m[b], &full[stage], s * kStripW,
+                       rt * kTileR, policy);
+      // the tile's 16 rows of the stage vector (the vector carries a zeroed
+      // tail of kVecPad entries, so the last tile never reads past it)
+      bulk_load(yrows + stage * kTileR, a.y + g.blk[b].row_off + rt * kTileR, kYRowBytes,
+                &full[stage]);
     }
     // Do not leave while a load is in flight: wait until every issued tile
     // was released by the consumers, or, if they gave up, until it landed.
@@ -148,13 +157,13 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
       }
     }
     const int r0 = rt * kTileR + 2 * warp;
-    const double2 yr0 = (r0 < bg.nrow) ? ld_y(a.y, bg.row_off + r0) : make_double2(0.0, 0.0);
-    const double2 yr1 =
-        (r0 + 1 < bg.nrow) ? ld_y(a.y, bg.row_off + r0 + 1) : make_double2(0.0, 0.0);
-
     const int stage = it % kStages;
     const int round = it / kStages;
     if (!dead && !mbar_wait_bounded(&full[stage], round & 1, a.status)) dead = true;
+    // rows past the block's end meet zero-filled dipole rows, so their
+    // (finite) stage-vector entries contribute nothing
+    const double2 yr0 = dead ? make_double2(0.0, 0.0) : yrows[stage * kTileR + 2 * warp];
+    const double2 yr1 = dead ? make_double2(0.0, 0.0) : yrows[stage * kTileR + 2 * warp + 1];
     const double* T = tiles + stage * (kTileR * kStripW);
     const double* T0 = T + (2 * warp) * kStripW + 2 * lane;
     const double* T1 = T0 + kStripW;
