@@ -51,6 +51,8 @@ __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a,
 __global__ void __launch_bounds__(kCombineThreads)
     k_stage_combine(const __grid_constant__ CombineArgs a) {
   const Geometry& g = a.g;
+  pdl_trigger();
+  pdl_wait();
   // kCombineLanes consecutive threads share one coefficient: they split its
   // partial sums (strip s and slot s handled by lane s mod kCombineLanes) and
   // reduce them with a fixed shuffle tree; lane 0 finishes the coefficient.
@@ -156,6 +158,8 @@ struct RenormArgs {
 
 __global__ void __launch_bounds__(kCombineThreads) k_renorm(const __grid_constant__ RenormArgs a) {
   __shared__ double nrm_sh;
+  pdl_trigger();
+  pdl_wait();
   if (threadIdx.x < 32) {
     double s = 0.0;
     for (int p = threadIdx.x; p < a.nparts; p += 32) s += a.norm_part[p];

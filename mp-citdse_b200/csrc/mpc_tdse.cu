@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -234,11 +235,40 @@ struct ProfScope {
 
 // --- launch sequences -------------------------------------------------------
 
+// Launches with programmatic stream serialization: the kernel may be
+// scheduled while the previous kernel on the stream is still running; each
+// kernel calls pdl_wait() before touching data an earlier kernel produced.
+// MPC_NO_PDL=1 in the environment turns it off (plain stream order), a
+// debugging aid.
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("MPC_NO_PDL");
+    return !(e && e[0] == '1');
+  }();
+  return on;
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem,
+                       cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 int launch_stream(mpc_ctx* c, const double2* y) {
   c->sargs.y = y;
   ProfScope ps(c, MPC_KERNEL_RHS_STREAM);
-  k_rhs_stream<<<c->stream_grid, kStreamThreads, kStreamSmem, c->stream>>>(c->sargs, c->tmaps);
-  CK(cudaGetLastError());
+  CK(launch_pdl(k_rhs_stream, c->stream_grid, kStreamThreads, kStreamSmem, c->stream, c->sargs,
+                c->tmaps));
   return MPC_OK;
 }
 
@@ -272,8 +302,7 @@ int launch_combine(mpc_ctx* c, int stage, int step, double dt, const double2* y,
   }
   a.g = c->g;
   ProfScope ps(c, MPC_KERNEL_COMBINE);
-  k_stage_combine<<<c->combine_grid, kCombineThreads, 0, c->stream>>>(a);
-  CK(cudaGetLastError());
+  CK(launch_pdl(k_stage_combine, c->combine_grid, kCombineThreads, 0, c->stream, a));
   return MPC_OK;
 }
 
@@ -290,8 +319,7 @@ int launch_renorm(mpc_ctx* c, int step, int pop_index) {
   r.norm_hist = c->d_nrm;
   r.status = c->d_status;
   ProfScope ps(c, MPC_KERNEL_RENORM);
-  k_renorm<<<c->combine_grid, kCombineThreads, 0, c->stream>>>(r);
-  CK(cudaGetLastError());
+  CK(launch_pdl(k_renorm, c->combine_grid, kCombineThreads, 0, c->stream, r));
   return MPC_OK;
 }
 

@@ -73,22 +73,43 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
     fence_mbar_init();
   }
   __syncthreads();
-  if (t_begin >= t_end) return;
+  pdl_trigger();
+  if (t_begin >= t_end) {
+    pdl_wait();
+    return;
+  }
 
   if (warp == kConsumerWarps) {
     // ---------------- producer ----------------
-    if (lane != 0) return;
+    if (lane != 0) {
+      pdl_wait();
+      return;
+    }
     const uint64_t policy = make_evict_first_policy();
+    // The dipole blocks do not change between launches: the first ring's
+    // worth of tiles is requested before waiting for the previous kernel;
+    // their stage-vector rows (written by that kernel) only after it.
+    const int pre = (t_end - t_begin < kStages) ? (t_end - t_begin) : kStages;
+    for (int i = 0; i < pre; ++i) {
+      int b, s, rt;
+      decode_tile(g, t_begin + i, b, s, rt);
+      mbar_arrive_expect_tx(&full[i], kTileBytes + kYRowBytes);
+      tma_load_2d_hint(tiles + i * (kTileR * kStripW), &tm.m[b], &full[i], s * kStripW,
+                       rt * kTileR, policy);
+    }
+    pdl_wait();
     int issued = 0;
     for (int t = t_begin; t < t_end; ++t, ++issued) {
       const int stage = issued % kStages;
       const int round = issued / kStages;
-      if (round > 0 && !mbar_wait_bounded(&empty[stage], (round - 1) & 1, a.status)) break;
       int b, s, rt;
       decode_tile(g, t, b, s, rt);
-      mbar_arrive_expect_tx(&full[stage], kTileBytes + kYRowBytes);
-      tma_load_2d_hint(tiles + stage * (kTileR * kStripW), &tm.m[b], &full[stage], s * kStripW,
-                       rt * kTileR, policy);
+      if (issued >= pre) {
+        if (!mbar_wait_bounded(&empty[stage], (round - 1) & 1, a.status)) break;
+        mbar_arrive_expect_tx(&full[stage], kTileBytes + kYRowBytes);
+        tma_load_2d_hint(tiles + stage * (kTileR * kStripW), &tm.m[b], &full[stage],
+                         s * kStripW, rt * kTileR, policy);
+      }
       // the tile's 16 rows of the stage vector (the vector carries a zeroed
       // tail of kVecPad entries, so the last tile never reads past it)
       bulk_load(yrows + stage * kTileR, a.y + g.blk[b].row_off + rt * kTileR, kYRowBytes,
@@ -106,6 +127,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   }
 
   // ---------------- consumers ----------------
+  pdl_wait();
   double2 ycol[8];
   double2 cacc[8];
   int cur_b = -1, cur_s = -1;
