@@ -125,6 +125,30 @@ int mpc_advance(mpc_ctx *ctx, const mpc_pulse *pulse, double t0, double dt, int 
 int mpc_history_get(mpc_ctx *ctx, int steps, double *pop_out, double *field_out,
                     double *norm_out);
 
+/* Batched right-hand side (new: the reference evaluates one state at a
+ * time): B states x [B][2*size] (host, each state contiguous) at fields
+ * F[B]; dxdt [B][2*size].  The coupling is applied as one FP64 tensor-core
+ * GEMM over all B states. */
+int mpc_batch_rhs(mpc_ctx *ctx, int B, const double *F, const double *x, double *dxdt);
+
+/* Batched adaptive RKF78 (new: the reference propagates one pulse per run,
+ * with a fixed step).  B pulses, each with its own field (pulses[b]), start
+ * time t0[b] and end time t_end[b], advance together on the GPU; each has
+ * its own step size and accept/reject history:
+ *   stage fields F_b(t + c_s h) (continuous field), 8th-order solution,
+ *   embedded 7th-order error e, err = max_i |e_i| / (atol + rtol *
+ *   max(|x_i|, |x_new_i|)), accept if err <= 1, then x = x_new / ||x_new||;
+ *   next h = h * clamp(0.9 * err^(-1/8), 0.2, 5) (at most 1 after a
+ *   rejection), capped at dt_max and at t_end - t.
+ * ct: host [B][2*size] in/out.  accepted / rejected / t_final (host arrays of
+ * B, optional) receive each pulse's accepted and rejected step counts and
+ * end time.  max_attempts (<= 0: unlimited) bounds the attempts per pulse;
+ * a pulse that hits it stops and the call returns MPC_ERR_DEVICE. */
+int mpc_batch_propagate(mpc_ctx *ctx, int B, const mpc_pulse *pulses, const double *t0,
+                        const double *t_end, double h0, double dt_max, double rtol, double atol,
+                        int max_attempts, double *ct, int *accepted, int *rejected,
+                        double *t_final);
+
 /* Kernel timing (profiling aid).  While enabled, CUDA events on the
  * context's stream bracket every launch of each kernel kind:
  *   MPC_KERNEL_RHS_STREAM (0)  the dipole-block streaming pass,
@@ -135,6 +159,7 @@ int mpc_history_get(mpc_ctx *ctx, int steps, double *pop_out, double *field_out,
 #define MPC_KERNEL_RHS_STREAM 0
 #define MPC_KERNEL_COMBINE 1
 #define MPC_KERNEL_RENORM 2
+#define MPC_KERNEL_BATCH 3   /* every kernel of the batched path */
 int mpc_profile_enable(mpc_ctx *ctx, int on);
 int mpc_profile_read(mpc_ctx *ctx, int kind, double *total_ms, long long *launches);
 

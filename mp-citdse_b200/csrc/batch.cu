@@ -1,0 +1,857 @@
+// batch.cu -- many pulses in one propagation: batched adaptive RKF78.
+//
+// The reference propagates one pulse per process (tdse::propV / propL,
+// src/tdse/tdse.cpp:146-310) with a fixed step.  Here B pulses -- each with
+// its own field, duration, step size and accept/reject history -- advance
+// together.  The state of all pulses is one matrix X [n][B] (row = basis
+// state, complex column = pulse), so every right-hand side is a real GEMM of
+// the block-tridiagonal coupling (the dipole blocks) with the [n x 2B] stage
+// matrix, run on the FP64 tensor cores (mma.sync m16n8k8 .f64), with the RK
+// stage epilogue fused into the GEMM's store.
+//
+// Per attempted step (all active pulses at once):
+//   13 x k_batch_stage   (GEMM + epilogue: k_s, next stage input; the last
+//                         stage also forms x_new, the embedded 7th-order
+//                         error and per-pulse norm partials)
+//    1 x k_batch_control (per pulse: accept/reject, next step, stage fields)
+//    1 x k_batch_apply   (accepted pulses: x = x_new / ||x_new||; retired
+//                         pulses write their final state out)
+// Retired pulses' columns are compacted away so the GEMM narrows.
+// Step control and error norm are those of the CPU oracle's adaptive driver:
+//   err = max_i |e_i| / (atol + rtol*max(|x_i|, |x_new_i|)),
+//   factor = clamp(0.9 * err^(-1/8), 0.2, 5) with err^(-1/8) as
+//   1/sqrt(sqrt(sqrt(err))), stage fields F(t + c_s h) (continuous field).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "ctx.h"
+#include "dev_util.cuh"
+#include "plan.h"
+#include "rkf78.h"
+
+using namespace mpc;
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 32, NSTB = 3, BTHREADS = 128;
+constexpr int LDA_P = BM + 4;   // A stored [k][m] (transposed block), pitch in doubles
+constexpr int LDA_Q = BK + 4;   // A stored [m][k]
+constexpr int LDB = BN + 4;     // B stored [k][n]
+constexpr int A_STAGE = (BK * LDA_P > BM * LDA_Q) ? BK * LDA_P : BM * LDA_Q;
+constexpr int B_STAGE = BK * LDB;
+constexpr int BATCH_SMEM = NSTB * (A_STAGE + B_STAGE) * 8;
+constexpr int kColAlign = 32;   // pulse columns are allocated in multiples of this
+
+__constant__ double c_A[13][13];
+__constant__ double c_B8[13];
+__constant__ double c_E[13];   // b8 - b7
+__constant__ double c_C[13];
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = smem_u32(smem);
+  const int sz = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(sz)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// D (16x8, f64) += A (16x8) * B (8x8); fragments as in the PTX ISA for
+// m16n8k8 .f64: a = {A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]},
+// b = {B[t][g], B[t+4][g]}, c = {C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]}
+// with g = lane / 4, t = lane % 4.
+__device__ __forceinline__ void dmma16x8x8(double* c, const double* a, const double* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+__device__ double dev_field(const mpc_pulse& p, double t) {
+  const double Eo = p.Eo, w = p.w, cepd = p.cepd, a = p.a, b = p.b;
+  switch (p.kind) {
+    case MPC_FIELD_SINE_EE:
+    case MPC_FIELD_SINE_AA: {
+      const double s = sin(a * t);
+      return (double)(t >= 0.0 && t <= M_PI / a) * Eo * s * s * sin(w * t + cepd);
+    }
+    case MPC_FIELD_SINE_AE: {
+      const double Wt = a * t, s = sin(Wt), wtc = w * t + cepd;
+      return (double)(t >= 0.0 && t <= M_PI / a) * Eo *
+             (w * s * s * cos(wtc) + a * sin(2 * Wt) * sin(wtc));
+    }
+    case MPC_FIELD_SINE_EA: {
+      const double WpP = w + 2.0 * a, WpN = w - 2.0 * a;
+      return (double)(t >= 0.0 && t <= M_PI / a) * 0.5 * Eo *
+             (((1.0 - cos(w * t + cepd)) / w) -
+              0.5 * ((1.0 - cos(WpP * t)) / WpP + (1.0 - cos(WpN * t)) / WpN));
+    }
+    case MPC_FIELD_GAUSS: {
+      const double td = t - 0.5 * b;
+      return (double)(t >= 0.0 && t <= b) * Eo * exp(-td * td / (a * a)) * sin(w * t + cepd);
+    }
+  }
+  return 0.0;
+}
+
+struct StageArgs {
+  const double* D;
+  const double* eps;
+  const double2* X;      // x, [n][ldc]
+  const double2* Yin;    // y_s (X for s = 0)
+  double2* K;            // k[13][n][ldc]
+  double2* Yout;         // y_{s+1}, or x_new for s = 12
+  const double* Fs;      // [13][ldc] stage fields
+  const double* h;       // [ldc] attempt step
+  unsigned long long* err;  // [ldc] bits of the max error ratio
+  double* normpart;      // [nrowtiles][ldc]
+  double rtol, atol;
+  int stage;
+  int gauge;             // 0 length, 1 velocity
+  int ncol;              // active pulse columns
+  int ldc;               // allocated pulse columns (row pitch of X, Y, K in complex)
+  int nrowtiles;
+  int want_k_only;       // 1: stop after storing k_s (single RHS evaluations)
+  Geometry g;
+};
+
+__global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_constant__ StageArgs a) {
+  extern __shared__ __align__(16) double bsm[];
+  pdl_trigger();
+  const Geometry& g = a.g;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int wm = warp >> 1, wn = warp & 1;
+
+  // row tile -> state block L and first local row r0
+  int L = 0, rt = blockIdx.x;
+  while (true) {
+    const int nt = (g.state_off[L + 1] - g.state_off[L] + BM - 1) / BM;
+    if (rt < nt || L + 1 >= g.nstate_blk) break;
+    rt -= nt;
+    ++L;
+  }
+  const int nL = g.state_off[L + 1] - g.state_off[L];
+  const int r0 = rt * BM;
+  const int c0 = blockIdx.y * BN;           // first real column
+  const int ncr = 2 * a.ncol;               // real columns in use
+  const int ldr = 2 * a.ldc;                // real row pitch of X / Y
+  const bool hasP = L > 0, hasQ = L < g.nblk;
+  const int KP = hasP ? g.state_off[L] - g.state_off[L - 1] : 0;
+  const int KQ = hasQ ? g.state_off[L + 2] - g.state_off[L + 1] : 0;
+  const int nchP = (KP + BK - 1) / BK, nchQ = (KQ + BK - 1) / BK;
+  const int nch = nchP + nchQ;
+  const double qsign = (a.gauge == 1) ? -1.0 : 1.0;
+
+  pdl_wait();
+  const double* Yin = reinterpret_cast<const double*>(a.Yin);
+
+  auto load_chunk = [&](int ch, int st) {
+    double* As = bsm + st * (A_STAGE + B_STAGE);
+    double* Bs = As + A_STAGE;
+    const bool isP = ch < nchP;
+    const int k0 = (isP ? ch : ch - nchP) * BK;
+    const int nK = isP ? KP : KQ;
+    const int yrow0 = isP ? g.state_off[L - 1] : g.state_off[L + 1];
+    if (isP) {
+      // A = D_{L-1}^T : copy D_{L-1}[k0+kk][r0+mm] into As[kk][mm]
+      const BlockGeom& bb = g.blk[L - 1];
+      for (int e = threadIdx.x; e < BK * (BM / 2); e += BTHREADS) {
+        const int kk = e / (BM / 2), mm = 2 * (e % (BM / 2));
+        const bool v = (k0 + kk < nK) && (r0 + mm < nL);
+        const double* src = a.D + bb.d_off + (long long)(v ? k0 + kk : 0) * bb.pitch + (v ? r0 + mm : 0);
+        cp_async16(As + kk * LDA_P + mm, src, v);
+      }
+    } else {
+      // A = D_L : copy D_L[r0+mm][k0+kk] into As[mm][kk]
+      const BlockGeom& bb = g.blk[L];
+      for (int e = threadIdx.x; e < BM * (BK / 2); e += BTHREADS) {
+        const int mm = e / (BK / 2), kk = 2 * (e % (BK / 2));
+        const bool v = (r0 + mm < nL) && (k0 + kk < nK);
+        const double* src = a.D + bb.d_off + (long long)(v ? r0 + mm : 0) * bb.pitch + (v ? k0 + kk : 0);
+        cp_async16(As + mm * LDA_Q + kk, src, v);
+      }
+    }
+    // B = Y rows of the coupled block: Bs[kk][nn]
+    for (int e = threadIdx.x; e < BK * (BN / 2); e += BTHREADS) {
+      const int kk = e / (BN / 2), nn = 2 * (e % (BN / 2));
+      const bool v = (k0 + kk < nK) && (c0 + nn < ncr);
+      const double* src = Yin + (long long)(v ? yrow0 + k0 + kk : 0) * ldr + (v ? c0 + nn : 0);
+      cp_async16(Bs + kk * LDB + nn, src, v);
+    }
+  };
+
+  double acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+
+  for (int p = 0; p < NSTB - 1; ++p) {
+    if (p < nch) load_chunk(p, p);
+    cp_commit();
+  }
+  for (int ch = 0; ch < nch; ++ch) {
+    cp_wait<NSTB - 2>();
+    __syncthreads();
+    {
+      const int nx = ch + NSTB - 1;
+      if (nx < nch) load_chunk(nx, nx % NSTB);
+      cp_commit();
+    }
+    const int st = ch % NSTB;
+    const double* As = bsm + st * (A_STAGE + B_STAGE);
+    const double* Bs = As + A_STAGE;
+    const bool isP = ch < nchP;
+    const double sg = isP ? 1.0 : qsign;
+#pragma unroll
+    for (int ks = 0; ks < BK / 8; ++ks) {
+      double af[2][4], bf[4][2];
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        const int m = wm * 32 + mt * 16 + gq;
+        const int k = ks * 8 + tq;
+        if (isP) {
+          af[mt][0] = As[k * LDA_P + m];
+          af[mt][1] = As[k * LDA_P + m + 8];
+          af[mt][2] = As[(k + 4) * LDA_P + m];
+          af[mt][3] = As[(k + 4) * LDA_P + m + 8];
+        } else {
+          af[mt][0] = sg * As[m * LDA_Q + k];
+          af[mt][1] = sg * As[(m + 8) * LDA_Q + k];
+          af[mt][2] = sg * As[m * LDA_Q + k + 4];
+          af[mt][3] = sg * As[(m + 8) * LDA_Q + k + 4];
+        }
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int n = wn * 32 + nt * 8 + gq;
+        const int k = ks * 8 + tq;
+        bf[nt][0] = Bs[k * LDB + n];
+        bf[nt][1] = Bs[(k + 4) * LDB + n];
+      }
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) dmma16x8x8(acc[mt][nt], af[mt], bf[nt]);
+    }
+  }
+  cp_wait<0>();
+
+  // ---------------- fused RK epilogue ----------------
+  const int s = a.stage;
+  const long long nld = (long long)g.ntot * a.ldc;  // complex elements per k slab
+  const bool last = (s == kNumStages - 1);
+  __shared__ double red_n[2][BN / 2];
+  __shared__ double red_e[2][BN / 2];
+#pragma unroll
+  for (int nt = 0; nt < 4; ++nt) {
+    const int q = (c0 + wn * 32 + nt * 8) / 2 + tq;  // pulse column
+    const bool qv = q < a.ncol;
+    double nsum = 0.0, emax = 0.0;
+    const double F = qv ? a.Fs[s * a.ldc + q] : 0.0;
+    const double hq = qv ? a.h[q] : 0.0;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int hr = 0; hr < 2; ++hr) {
+        const int r = r0 + wm * 32 + mt * 16 + gq + 8 * hr;
+        if (!qv || r >= nL) continue;
+        const long long i = g.state_off[L] + r;
+        const long long idx = i * a.ldc + q;
+        const double wre = acc[mt][nt][2 * hr], wim = acc[mt][nt][2 * hr + 1];
+        const double2 y = a.Yin[idx];
+        const double e = a.eps[i];
+        double kre, kim;
+        if (a.gauge == 0) {
+          kre = fma(F, wim, e * y.y);
+          kim = -fma(F, wre, e * y.x);
+        } else {
+          kre = fma(F, wre, e * y.y);
+          kim = fma(F, wim, -e * y.x);
+        }
+        a.K[s * nld + idx] = make_double2(kre, kim);
+        if (a.want_k_only) continue;
+        const double2 x = a.X[idx];
+        double2 o = x;
+        if (!last) {
+#pragma unroll
+          for (int j = 0; j < kNumStages; ++j) {
+            const double cj = c_A[s + 1][j];
+            if (j > s || cj == 0.0) continue;
+            const double2 kj = (j == s) ? make_double2(kre, kim) : a.K[j * nld + idx];
+            const double cf = hq * cj;
+            o.x = fma(cf, kj.x, o.x);
+            o.y = fma(cf, kj.y, o.y);
+          }
+        } else {
+          double2 er = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int j = 0; j < kNumStages; ++j) {
+            const double bj = c_B8[j], ej = c_E[j];
+            if (bj == 0.0 && ej == 0.0) continue;
+            const double2 kj = (j == s) ? make_double2(kre, kim) : a.K[j * nld + idx];
+            if (bj != 0.0) {
+              o.x = fma(hq * bj, kj.x, o.x);
+              o.y = fma(hq * bj, kj.y, o.y);
+            }
+            if (ej != 0.0) {
+              er.x = fma(hq * ej, kj.x, er.x);
+              er.y = fma(hq * ej, kj.y, er.y);
+            }
+          }
+          const double ax = sqrt(x.x * x.x + x.y * x.y), an = sqrt(o.x * o.x + o.y * o.y);
+          const double ae = sqrt(er.x * er.x + er.y * er.y);
+          const double ratio = ae / (a.atol + a.rtol * fmax(ax, an));
+          emax = fmax(emax, ratio);
+          if (!(ratio == ratio)) emax = ratio;  // keep a NaN
+          nsum += o.x * o.x + o.y * o.y;
+        }
+        a.Yout[idx] = o;
+      }
+    if (last && !a.want_k_only) {
+      // per pulse: sum over this thread's rows, then over the 8 lanes sharing
+      // tq (fixed xor tree), then over the two warp rows (fixed order)
+#pragma unroll
+      for (int o = 4; o < 32; o <<= 1) {
+        nsum += __shfl_xor_sync(0xffffffffu, nsum, o);
+        const double oe = __shfl_xor_sync(0xffffffffu, emax, o);
+        emax = (oe != oe) ? oe : fmax(emax, oe);
+      }
+      const int col = wn * 16 + nt * 4 + tq;  // pulse slot within the CTA
+      if (gq == 0) {
+        red_n[wm][col] = nsum;
+        red_e[wm][col] = emax;
+      }
+    }
+  }
+  if (last && !a.want_k_only) {
+    __syncthreads();
+    if (threadIdx.x < BN / 2) {
+      const int q = c0 / 2 + threadIdx.x;
+      if (q < a.ncol) {
+        a.normpart[(long long)blockIdx.x * a.ldc + q] = red_n[0][threadIdx.x] + red_n[1][threadIdx.x];
+        const double e0 = red_e[0][threadIdx.x], e1 = red_e[1][threadIdx.x];
+        const double em = (e0 != e0) ? e0 : ((e1 != e1) ? e1 : fmax(e0, e1));
+        atomicMax(&a.err[q], (unsigned long long)__double_as_longlong(em));
+      }
+    }
+  }
+}
+
+// Per-pulse-column state.
+struct ColState {
+  mpc_pulse* pulse;
+  double* t;
+  double* t_end;
+  double* h;       // proposed next step
+  double* hatt;    // step of the current attempt
+  int* last;       // the attempt ends the pulse
+  int* done;
+  int* accepted;   // 1 if the last attempt was accepted
+  int* nacc;
+  int* nrej;
+  int* natt;
+  int* pulse_id;   // column -> pulse index
+  double* nrm;
+  int* retired;    // set when the pulse finishes; cleared once its state is out
+};
+
+// Per-pulse results, indexed by pulse id (columns move; these do not).
+struct PulseResults {
+  int* nacc;
+  int* nrej;
+  double* t;
+  int* status;     // 0 finished at t_end, 2 gave up after max_attempts
+};
+
+struct ControlArgs {
+  ColState c;
+  PulseResults res;
+  double* Fs;                 // [13][ldc]
+  unsigned long long* err;
+  const double* normpart;
+  int nrowtiles;
+  int ncol, ldc;
+  int mode;                   // 0: start, 1: after an attempt
+  double h0, dt_max;
+  int max_attempts;
+};
+
+__device__ void prepare_attempt(const ControlArgs& a, int q) {
+  const ColState& c = a.c;
+  if (c.done[q]) {
+    c.hatt[q] = 0.0;
+    for (int s = 0; s < kNumStages; ++s) a.Fs[s * a.ldc + q] = 0.0;
+    return;
+  }
+  double h = c.h[q];
+  const double rem = c.t_end[q] - c.t[q];
+  int last = 0;
+  if (h >= rem) {
+    h = rem;
+    last = 1;
+  }
+  c.hatt[q] = h;
+  c.last[q] = last;
+  const mpc_pulse p = c.pulse[q];
+  for (int s = 0; s < kNumStages; ++s) a.Fs[s * a.ldc + q] = dev_field(p, c.t[q] + c_C[s] * h);
+}
+
+__device__ void retire(const ControlArgs& a, int q) {
+  const ColState& c = a.c;
+  const int id = c.pulse_id[q];
+  a.res.nacc[id] = c.nacc[q];
+  a.res.nrej[id] = c.nrej[q];
+  a.res.t[id] = c.t[q];
+  a.res.status[id] = (c.done[q] == 2) ? 2 : 0;
+  c.retired[q] = 1;
+}
+
+__global__ void k_batch_control(const __grid_constant__ ControlArgs a) {
+  pdl_trigger();
+  pdl_wait();
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= a.ncol) return;
+  const ColState& c = a.c;
+  if (a.mode == 0) {
+    c.h[q] = a.h0;
+    c.done[q] = (c.t[q] >= c.t_end[q]) ? 1 : 0;
+    c.accepted[q] = 0;
+    c.retired[q] = 0;
+    a.err[q] = 0ull;
+    if (c.done[q]) retire(a, q);
+    prepare_attempt(a, q);
+    return;
+  }
+  c.accepted[q] = 0;
+  if (c.done[q]) return;
+  const double err = __longlong_as_double((long long)a.err[q]);
+  a.err[q] = 0ull;
+  double ns = 0.0;
+  for (int r = 0; r < a.nrowtiles; ++r) ns += a.normpart[(long long)r * a.ldc + q];
+  const double nrm = sqrt(ns);
+  const double hh = c.hatt[q];
+  const double safety = 0.9, facmin = 0.2, facmax = 5.0;
+  double fac;
+  if (err == 0.0) {
+    fac = facmax;
+  } else {
+    fac = safety / sqrt(sqrt(sqrt(err)));
+    fac = fmin(fmax(fac, facmin), facmax);
+  }
+  c.natt[q] += 1;
+  const bool ok = (err <= 1.0) && (nrm > 0.0) && isfinite(nrm);
+  if (ok) {
+    c.t[q] = c.last[q] ? c.t_end[q] : c.t[q] + hh;
+    c.nacc[q] += 1;
+    c.accepted[q] = 1;
+    c.nrm[q] = nrm;
+    double hn = hh * fac;
+    if (hn > a.dt_max) hn = a.dt_max;
+    c.h[q] = hn;
+    if (c.last[q]) c.done[q] = 1;
+  } else {
+    c.nrej[q] += 1;
+    c.h[q] = hh * fmin(fac, 1.0);
+  }
+  // give up after max_attempts, or when rejections have shrunk the step to
+  // nothing (a non-finite error keeps rejecting)
+  if (!c.done[q] && (c.natt[q] >= a.max_attempts ||
+                     c.h[q] < 1e-13 * fmax(1.0, fabs(c.t_end[q]))))
+    c.done[q] = 2;
+  if (c.done[q]) retire(a, q);
+  prepare_attempt(a, q);
+}
+
+struct ApplyArgs {
+  double2* X;
+  const double2* Xn;
+  ColState c;
+  double2* out;     // [B][n] final states (user layout)
+  int ntot, ncol, ldc;
+};
+
+__global__ void k_batch_apply(const __grid_constant__ ApplyArgs a) {
+  pdl_trigger();
+  pdl_wait();
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long tot = (long long)a.ntot * a.ncol;
+  if (e >= tot) return;
+  const int i = (int)(e / a.ncol), q = (int)(e % a.ncol);
+  const long long idx = (long long)i * a.ldc + q;
+  double2 o;
+  if (a.c.accepted[q]) {
+    const double2 v = a.Xn[idx];
+    const double nrm = a.c.nrm[q];
+    o = make_double2(v.x / nrm, v.y / nrm);
+    a.X[idx] = o;
+  } else {
+    if (!a.c.retired[q]) return;
+    o = a.X[idx];
+  }
+  if (a.c.retired[q]) a.out[(long long)a.c.pulse_id[q] * a.ntot + i] = o;
+}
+
+// Clears the retired flags once apply has written the states out.
+__global__ void k_batch_clear_retired(int* retired, int ncol) {
+  pdl_trigger();
+  pdl_wait();
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < ncol) retired[q] = 0;
+}
+
+// X columns in from the user layout [B][n].
+__global__ void k_batch_load(double2* X, const double2* in, int ntot, int ncol, int ldc) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)ntot * ncol) return;
+  const int i = (int)(e / ncol), q = (int)(e % ncol);
+  X[(long long)i * ldc + q] = in[(long long)q * ntot + i];
+}
+
+// Compaction: column q of the new layout takes column map[q] of the old.
+__global__ void k_batch_gather_cols(double2* dst, const double2* src, const int* map, int ntot,
+                                    int ncol, int ldc) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)ntot * ncol) return;
+  const int i = (int)(e / ncol), q = (int)(e % ncol);
+  dst[(long long)i * ldc + q] = src[(long long)i * ldc + map[q]];
+}
+
+// K slabs of a single RHS evaluation out to the user layout [B][n].
+__global__ void k_batch_store_k0(double2* out, const double2* K, int ntot, int ncol, int ldc) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)ntot * ncol) return;
+  const int i = (int)(e / ncol), q = (int)(e % ncol);
+  out[(long long)q * ntot + i] = K[(long long)i * ldc + q];
+}
+
+template <class T>
+__global__ void k_gather_scalar(T* dst, const T* src, const int* map, int n) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) dst[q] = src[map[q]];
+}
+
+}  // namespace
+
+struct mpc_batch_state {
+  int ldc = 0;        // allocated pulse columns
+  int nrowtiles = 0;
+  double2* X = nullptr;
+  double2* Y[2] = {nullptr, nullptr};
+  double2* K = nullptr;
+  double2* out = nullptr;   // [ldc][n] user layout
+  double* Fs = nullptr;
+  unsigned long long* err = nullptr;
+  double* normpart = nullptr;
+  int* map = nullptr;
+  void* scratch = nullptr;  // compaction staging for per-column scalars
+  ColState c{};
+  PulseResults res{};
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+template <class T>
+int balloc(mpc_batch_state* b, T** p, size_t count) {
+  void* q = nullptr;
+  CK(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)));
+  b->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return MPC_OK;
+}
+
+int ensure_batch(mpc_ctx* c, int B) {
+  static bool consts = false;
+  if (!consts) {
+    double A[13][13], B8[13], E[13], Cn[13];
+    for (int i = 0; i < 13; ++i) {
+      for (int j = 0; j < 13; ++j) A[i][j] = rkf78::A[i][j];
+      B8[i] = rkf78::B8[i];
+      E[i] = rkf78::B8[i] - rkf78::B7[i];
+      Cn[i] = rkf78::C[i];
+    }
+    CK(cudaMemcpyToSymbol(c_A, A, sizeof A));
+    CK(cudaMemcpyToSymbol(c_B8, B8, sizeof B8));
+    CK(cudaMemcpyToSymbol(c_E, E, sizeof E));
+    CK(cudaMemcpyToSymbol(c_C, Cn, sizeof Cn));
+    CK(cudaFuncSetAttribute(k_batch_stage, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            BATCH_SMEM));
+    consts = true;
+  }
+  const int ldc = (B + kColAlign - 1) / kColAlign * kColAlign;
+  if (c->batch && c->batch->ldc >= ldc) return MPC_OK;
+  mpc_batch_free(c);
+  mpc_batch_state* b = new mpc_batch_state();
+  c->batch = b;
+  b->ldc = ldc;
+  const Geometry& g = c->g;
+  int nrt = 0;
+  for (int L = 0; L < g.nstate_blk; ++L)
+    nrt += (g.state_off[L + 1] - g.state_off[L] + BM - 1) / BM;
+  b->nrowtiles = nrt;
+  const size_t nel = (size_t)g.ntot * ldc;
+  int rc;
+  ColState& s = b->c;
+  if ((rc = balloc(b, &b->X, nel)) || (rc = balloc(b, &b->Y[0], nel)) ||
+      (rc = balloc(b, &b->Y[1], nel)) || (rc = balloc(b, &b->K, nel * kNumStages)) ||
+      (rc = balloc(b, &b->out, nel)) || (rc = balloc(b, &b->Fs, (size_t)kNumStages * ldc)) ||
+      (rc = balloc(b, &b->err, ldc)) || (rc = balloc(b, &b->normpart, (size_t)nrt * ldc)) ||
+      (rc = balloc(b, &b->map, ldc)) ||
+      (rc = balloc(b, reinterpret_cast<char**>(&b->scratch), sizeof(mpc_pulse) * ldc)) ||
+      (rc = balloc(b, &s.pulse, ldc)) || (rc = balloc(b, &s.t, ldc)) ||
+      (rc = balloc(b, &s.t_end, ldc)) || (rc = balloc(b, &s.h, ldc)) ||
+      (rc = balloc(b, &s.hatt, ldc)) || (rc = balloc(b, &s.last, ldc)) ||
+      (rc = balloc(b, &s.done, ldc)) || (rc = balloc(b, &s.accepted, ldc)) ||
+      (rc = balloc(b, &s.nacc, ldc)) || (rc = balloc(b, &s.nrej, ldc)) ||
+      (rc = balloc(b, &s.natt, ldc)) || (rc = balloc(b, &s.pulse_id, ldc)) ||
+      (rc = balloc(b, &s.nrm, ldc)) || (rc = balloc(b, &s.retired, ldc)) ||
+      (rc = balloc(b, &b->res.nacc, ldc)) || (rc = balloc(b, &b->res.nrej, ldc)) ||
+      (rc = balloc(b, &b->res.t, ldc)) || (rc = balloc(b, &b->res.status, ldc)))
+    return rc;
+  CK(cudaMemset(b->X, 0, nel * sizeof(double2)));
+  CK(cudaMemset(b->Y[0], 0, nel * sizeof(double2)));
+  CK(cudaMemset(b->Y[1], 0, nel * sizeof(double2)));
+  CK(cudaMemset(b->K, 0, nel * kNumStages * sizeof(double2)));
+  return MPC_OK;
+}
+
+StageArgs stage_args(mpc_ctx* c, int s, int ncol, double rtol, double atol, bool k_only) {
+  mpc_batch_state* b = c->batch;
+  StageArgs a{};
+  a.D = c->d_D;
+  a.eps = c->d_eps;
+  a.X = b->X;
+  a.Yin = (s == 0) ? b->X : b->Y[s & 1];
+  a.K = b->K;
+  a.Yout = b->Y[(s + 1) & 1];
+  a.Fs = b->Fs;
+  a.h = b->c.hatt;
+  a.err = b->err;
+  a.normpart = b->normpart;
+  a.rtol = rtol;
+  a.atol = atol;
+  a.stage = s;
+  a.gauge = (c->gauge == 'l') ? 0 : 1;
+  a.ncol = ncol;
+  a.ldc = b->ldc;
+  a.nrowtiles = b->nrowtiles;
+  a.want_k_only = k_only ? 1 : 0;
+  a.g = c->g;
+  return a;
+}
+
+int launch_stage(mpc_ctx* c, const StageArgs& a) {
+  ProfScope ps(c, 3);
+  const dim3 grid(a.nrowtiles, (2 * a.ncol + BN - 1) / BN);
+  CK(mpc_launch_pdl(k_batch_stage, grid, dim3(BTHREADS), BATCH_SMEM, c->stream, a));
+  return MPC_OK;
+}
+
+inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+void mpc_batch_free(mpc_ctx* c) {
+  if (!c || !c->batch) return;
+  for (void* p : c->batch->allocs) cudaFree(p);
+  delete c->batch;
+  c->batch = nullptr;
+}
+
+extern "C" {
+
+int mpc_batch_rhs(mpc_ctx* c, int B, const double* F, const double* x, double* dxdt) {
+  if (!c || !F || !x || !dxdt || B <= 0) return mpc_fail(MPC_ERR_ARG, "bad argument");
+  CK(cudaSetDevice(c->device));
+  int rc;
+  if ((rc = ensure_batch(c, B))) return rc;
+  mpc_batch_state* b = c->batch;
+  const int n = c->g.ntot;
+  CK(cudaMemcpyAsync(b->out, x, sizeof(double2) * (size_t)n * B, cudaMemcpyHostToDevice,
+                     c->stream));
+  k_batch_load<<<blocks_for((long long)n * B, 256), 256, 0, c->stream>>>(b->X, b->out, n, B, b->ldc);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(b->Fs, F, sizeof(double) * B, cudaMemcpyHostToDevice, c->stream));
+  if ((rc = launch_stage(c, stage_args(c, 0, B, 0.0, 0.0, true)))) return rc;
+  k_batch_store_k0<<<blocks_for((long long)n * B, 256), 256, 0, c->stream>>>(b->out, b->K, n, B,
+                                                                            b->ldc);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(dxdt, b->out, sizeof(double2) * (size_t)n * B, cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return MPC_OK;
+}
+
+int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0,
+                        const double* t_end, double h0, double dt_max, double rtol, double atol,
+                        int max_attempts, double* ct, int* accepted, int* rejected,
+                        double* t_final) {
+  if (!c || !pulses || !t0 || !t_end || !ct || B <= 0)
+    return mpc_fail(MPC_ERR_ARG, "bad argument");
+  if (!(h0 > 0.0) || !(dt_max > 0.0) || !(rtol >= 0.0) || !(atol >= 0.0) || rtol + atol <= 0.0)
+    return mpc_fail(MPC_ERR_ARG, "bad step-control parameters");
+  if (h0 * c->eps_max > kRk78ImagStability * 4.0 || dt_max * c->eps_max > kRk78ImagStability)
+    return mpc_fail(MPC_ERR_UNSTABLE,
+                    "dt_max*max|E| = %.4g exceeds the RKF78 imaginary-axis stability bound %.4g",
+                    dt_max * c->eps_max, kRk78ImagStability);
+  CK(cudaSetDevice(c->device));
+  int rc;
+  if ((rc = ensure_batch(c, B))) return rc;
+  mpc_batch_state* b = c->batch;
+  ColState& s = b->c;
+  const int n = c->g.ntot;
+  const int ldc = b->ldc;
+
+  // per-column start state
+  std::vector<int> ids(B);
+  for (int i = 0; i < B; ++i) ids[i] = i;
+  std::vector<int> zeros(B, 0);
+  CK(cudaMemcpyAsync(s.pulse, pulses, sizeof(mpc_pulse) * B, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s.t, t0, sizeof(double) * B, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s.t_end, t_end, sizeof(double) * B, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s.pulse_id, ids.data(), sizeof(int) * B, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s.nacc, zeros.data(), sizeof(int) * B, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s.nrej, zeros.data(), sizeof(int) * B, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s.natt, zeros.data(), sizeof(int) * B, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(b->out, ct, sizeof(double2) * (size_t)n * B, cudaMemcpyHostToDevice,
+                     c->stream));
+  k_batch_load<<<blocks_for((long long)n * B, 256), 256, 0, c->stream>>>(b->X, b->out, n, B, ldc);
+  CK(cudaGetLastError());
+
+  ControlArgs ca{};
+  ca.c = s;
+  ca.res = b->res;
+  ca.Fs = b->Fs;
+  ca.err = b->err;
+  ca.normpart = b->normpart;
+  ca.nrowtiles = b->nrowtiles;
+  ca.ldc = ldc;
+  ca.h0 = h0;
+  ca.dt_max = dt_max;
+  ca.max_attempts = max_attempts > 0 ? max_attempts : 1000000000;
+  ApplyArgs aa{};
+  aa.X = b->X;
+  aa.Xn = b->Y[1];
+  aa.c = s;
+  aa.out = b->out;
+  aa.ntot = n;
+  aa.ldc = ldc;
+
+  int ncol = B;
+  ca.ncol = ncol;
+  ca.mode = 0;
+  k_batch_control<<<blocks_for(ncol, 128), 128, 0, c->stream>>>(ca);
+  CK(cudaGetLastError());
+  ca.mode = 1;
+
+  std::vector<int> done_h(B), map_h(B);
+  std::vector<int> col_ids = ids;  // host mirror of pulse_id per column
+  const int check_every = 8;
+  for (long long it = 0;; ++it) {
+    for (int st = 0; st < kNumStages; ++st)
+      if ((rc = launch_stage(c, stage_args(c, st, ncol, rtol, atol, false)))) return rc;
+    ca.ncol = ncol;
+    {
+      ProfScope ps(c, 3);
+      CK(mpc_launch_pdl(k_batch_control, dim3(blocks_for(ncol, 128)), dim3(128), 0, c->stream, ca));
+    }
+    aa.ncol = ncol;
+    {
+      ProfScope ps(c, 3);
+      CK(mpc_launch_pdl(k_batch_apply, dim3(blocks_for((long long)n * ncol, 256)), dim3(256), 0,
+                        c->stream, aa));
+    }
+    {
+      ProfScope ps(c, 3);
+      CK(mpc_launch_pdl(k_batch_clear_retired, dim3(blocks_for(ncol, 128)), dim3(128), 0,
+                        c->stream, s.retired, ncol));
+    }
+    if ((it + 1) % check_every) continue;
+    CK(cudaMemcpyAsync(done_h.data(), s.done, sizeof(int) * ncol, cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    int act = 0;
+    for (int q = 0; q < ncol; ++q)
+      if (!done_h[q]) map_h[act++] = q;
+    if (act == 0) break;
+    // compact when at least one GEMM column tile (32 pulses) can be dropped
+    const int tiles_now = (2 * ncol + BN - 1) / BN, tiles_new = (2 * act + BN - 1) / BN;
+    if (tiles_new < tiles_now) {
+      CK(cudaMemcpyAsync(b->map, map_h.data(), sizeof(int) * act, cudaMemcpyHostToDevice,
+                         c->stream));
+      const int gb = blocks_for((long long)n * act, 256);
+      k_batch_gather_cols<<<gb, 256, 0, c->stream>>>(b->Y[0], b->X, b->map, n, act, ldc);
+      CK(cudaMemcpyAsync(b->X, b->Y[0], sizeof(double2) * (size_t)n * ldc,
+                         cudaMemcpyDeviceToDevice, c->stream));
+      const int sb = blocks_for(act, 128);
+#define GATHER(field, T)                                                                    \
+  k_gather_scalar<T><<<sb, 128, 0, c->stream>>>(reinterpret_cast<T*>(b->scratch), s.field,  \
+                                               b->map, act);                               \
+  CK(cudaMemcpyAsync(s.field, b->scratch, sizeof(T) * act, cudaMemcpyDeviceToDevice, c->stream));
+      GATHER(pulse, mpc_pulse)
+      GATHER(t, double)
+      GATHER(t_end, double)
+      GATHER(h, double)
+      GATHER(hatt, double)
+      GATHER(last, int)
+      GATHER(done, int)
+      GATHER(accepted, int)
+      GATHER(nacc, int)
+      GATHER(nrej, int)
+      GATHER(natt, int)
+      GATHER(pulse_id, int)
+      GATHER(nrm, double)
+      GATHER(retired, int)
+      for (int st = 0; st < kNumStages; ++st) {
+        k_gather_scalar<double><<<sb, 128, 0, c->stream>>>(reinterpret_cast<double*>(b->scratch),
+                                                           b->Fs + st * ldc, b->map, act);
+        CK(cudaMemcpyAsync(b->Fs + st * ldc, b->scratch, sizeof(double) * act,
+                           cudaMemcpyDeviceToDevice, c->stream));
+      }
+#undef GATHER
+      CK(cudaGetLastError());
+      // results of pulses retired earlier are already in `out`; keep the host
+      // mirror of the column -> pulse map for the final read-back
+      std::vector<int> nid(act);
+      for (int q = 0; q < act; ++q) nid[q] = col_ids[map_h[q]];
+      col_ids = nid;
+      ncol = act;
+    }
+  }
+  // per-pulse results (indexed by pulse id) and final states
+  std::vector<int> na(B), nr(B), stt(B);
+  std::vector<double> tf(B);
+  CK(cudaMemcpyAsync(na.data(), b->res.nacc, sizeof(int) * B, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(nr.data(), b->res.nrej, sizeof(int) * B, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(tf.data(), b->res.t, sizeof(double) * B, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(stt.data(), b->res.status, sizeof(int) * B, cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaMemcpyAsync(ct, b->out, sizeof(double2) * (size_t)n * B, cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  (void)col_ids;
+  int gave_up = 0;
+  for (int i = 0; i < B; ++i) {
+    if (accepted) accepted[i] = na[i];
+    if (rejected) rejected[i] = nr[i];
+    if (t_final) t_final[i] = tf[i];
+    gave_up += stt[i] == 2;
+  }
+  if (gave_up)
+    return mpc_fail(MPC_ERR_DEVICE, "%d pulse(s) stopped after max_attempts step attempts",
+                    gave_up);
+  return MPC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,98 @@
+// ctx.h -- the context object shared by the library's translation units,
+// and its error helpers.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/mpc_tdse.h"
+#include "plan.h"
+#include "stream_types.h"
+
+// Records `fmt` as the calling thread's last error and returns `code`.
+int mpc_fail(int code, const char* fmt, ...);
+int mpc_internal_fail(int code, const char* msg);
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return mpc_fail(e_ == cudaErrorMemoryAllocation ? MPC_ERR_NOMEM : MPC_ERR_CUDA,    \
+                      "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,  \
+                      __LINE__);                                                         \
+  } while (0)
+
+struct mpc_batch_state;
+
+struct mpc_ctx {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  char gauge = 'l';
+  mpc::Geometry g{};
+  std::vector<int> n;
+  double eps_max = 0.0;
+
+  // device buffers
+  double* d_eps = nullptr;
+  double* d_D = nullptr;
+  double2* d_x = nullptr;
+  double2* d_y = nullptr;
+  double2* d_k = nullptr;
+  double2* d_RP = nullptr;
+  double2* d_CP = nullptr;
+  int* d_cta_slot0 = nullptr;
+  int* d_strip_slot0 = nullptr;
+  double* d_norm_part = nullptr;
+  unsigned* d_status = nullptr;
+  double* d_Ftab = nullptr;
+  double* d_pop = nullptr;
+  double* d_nrm = nullptr;
+  int hist_cap = 0;
+
+  // profiling: event pairs per kernel kind, and a launch counter
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[4];
+  std::vector<cudaEvent_t> ev_pool;
+  long long launches = 0;
+
+  int stream_grid = 0;
+  int combine_grid = 0;
+  mpc::TmapSet tmaps{};
+  mpc::StreamArgs sargs{};
+  std::vector<void*> allocs;
+
+  mpc_batch_state* batch = nullptr;  // batched-propagation work space (batch.cu)
+};
+
+// Launch with programmatic stream serialization (see mpc_tdse.cu).
+bool mpc_pdl_enabled();
+template <typename... KArgs, typename... Args>
+cudaError_t mpc_launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                           cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = mpc_pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
+// Event bracket for profiling one launch of kernel kind `kind`.
+struct ProfScope {
+  mpc_ctx* c;
+  int kind;
+  cudaEvent_t b = nullptr;
+  ProfScope(mpc_ctx* c_, int k);
+  ~ProfScope();
+};
+
+void mpc_batch_free(mpc_ctx* c);

@@ -15,6 +15,7 @@
 
 #include "../../include/mpc_tdse.h"
 #include "combine.cuh"
+#include "ctx.h"
 #include "plan.h"
 #include "rhs_stream.cuh"
 #include "rkf78.h"
@@ -36,59 +37,18 @@ static int fail(int code, const char* fmt, ...) {
   return code;
 }
 
+int mpc_fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
 // error reporting for the other translation units of the library
 int mpc_internal_fail(int code, const char* msg) { return fail(code, "%s", msg); }
-
-#define CK(call)                                                                         \
-  do {                                                                                   \
-    cudaError_t e_ = (call);                                                             \
-    if (e_ != cudaSuccess)                                                               \
-      return fail(e_ == cudaErrorMemoryAllocation ? MPC_ERR_NOMEM : MPC_ERR_CUDA,        \
-                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,      \
-                  __LINE__);                                                             \
-  } while (0)
-
-// ---------------------------------------------------------------------------
-// context
-// ---------------------------------------------------------------------------
-struct mpc_ctx {
-  int device = 0;
-  int num_sms = 0;
-  cudaStream_t stream = nullptr;
-  char gauge = 'l';
-  Geometry g{};
-  std::vector<int> n;
-  double eps_max = 0.0;
-
-  // device buffers
-  double* d_eps = nullptr;
-  double* d_D = nullptr;
-  double2* d_x = nullptr;
-  double2* d_y = nullptr;
-  double2* d_k = nullptr;
-  double2* d_RP = nullptr;
-  double2* d_CP = nullptr;
-  int* d_cta_slot0 = nullptr;
-  int* d_strip_slot0 = nullptr;
-  double* d_norm_part = nullptr;
-  unsigned* d_status = nullptr;
-  double* d_Ftab = nullptr;
-  double* d_pop = nullptr;
-  double* d_nrm = nullptr;
-  int hist_cap = 0;
-
-  // profiling: event pairs per kernel kind, and a launch counter
-  bool profiling = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[3];
-  std::vector<cudaEvent_t> ev_pool;
-  long long launches = 0;
-
-  int stream_grid = 0;
-  int combine_grid = 0;
-  TmapSet tmaps{};
-  StreamArgs sargs{};
-  std::vector<void*> allocs;
-};
 
 namespace {
 
@@ -213,34 +173,33 @@ cudaEvent_t pool_get(mpc_ctx* c) {
   return e;
 }
 
-struct ProfScope {
-  mpc_ctx* c;
-  int kind;
-  cudaEvent_t b = nullptr;
-  ProfScope(mpc_ctx* c_, int k) : c(c_), kind(k) {
-    ++c->launches;
-    if (c->profiling) {
-      b = pool_get(c);
-      cudaEventRecord(b, c->stream);
-    }
+}  // namespace
+
+ProfScope::ProfScope(mpc_ctx* c_, int k) : c(c_), kind(k) {
+  ++c->launches;
+  if (c->profiling) {
+    b = pool_get(c);
+    cudaEventRecord(b, c->stream);
   }
-  ~ProfScope() {
-    if (b) {
-      cudaEvent_t e = pool_get(c);
-      cudaEventRecord(e, c->stream);
-      c->ev[kind].emplace_back(b, e);
-    }
+}
+
+ProfScope::~ProfScope() {
+  if (b) {
+    cudaEvent_t e = pool_get(c);
+    cudaEventRecord(e, c->stream);
+    c->ev[kind].emplace_back(b, e);
   }
-};
+}
+
+namespace {
 
 // --- launch sequences -------------------------------------------------------
 
-// Launches with programmatic stream serialization: the kernel may be
-// scheduled while the previous kernel on the stream is still running; each
-// kernel calls pdl_wait() before touching data an earlier kernel produced.
-// MPC_NO_PDL=1 in the environment turns it off (plain stream order), a
-// debugging aid.
-bool pdl_enabled() {
+// MPC_NO_PDL=1 in the environment turns programmatic dependent launch off
+// (plain stream order), a debugging aid.
+}  // namespace
+
+bool mpc_pdl_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("MPC_NO_PDL");
     return !(e && e[0] == '1');
@@ -248,27 +207,13 @@ bool pdl_enabled() {
   return on;
 }
 
-template <typename... KArgs, typename... Args>
-cudaError_t launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem,
-                       cudaStream_t st, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(block);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = pdl_enabled() ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, kern, args...);
-}
+namespace {
 
 int launch_stream(mpc_ctx* c, const double2* y) {
   c->sargs.y = y;
   ProfScope ps(c, MPC_KERNEL_RHS_STREAM);
-  CK(launch_pdl(k_rhs_stream, c->stream_grid, kStreamThreads, kStreamSmem, c->stream, c->sargs,
-                c->tmaps));
+  CK(mpc_launch_pdl(k_rhs_stream, dim3(c->stream_grid), dim3(kStreamThreads), kStreamSmem,
+                    c->stream, c->sargs, c->tmaps));
   return MPC_OK;
 }
 
@@ -302,7 +247,7 @@ int launch_combine(mpc_ctx* c, int stage, int step, double dt, const double2* y,
   }
   a.g = c->g;
   ProfScope ps(c, MPC_KERNEL_COMBINE);
-  CK(launch_pdl(k_stage_combine, c->combine_grid, kCombineThreads, 0, c->stream, a));
+  CK(mpc_launch_pdl(k_stage_combine, dim3(c->combine_grid), dim3(kCombineThreads), 0, c->stream, a));
   return MPC_OK;
 }
 
@@ -319,7 +264,7 @@ int launch_renorm(mpc_ctx* c, int step, int pop_index) {
   r.norm_hist = c->d_nrm;
   r.status = c->d_status;
   ProfScope ps(c, MPC_KERNEL_RENORM);
-  CK(launch_pdl(k_renorm, c->combine_grid, kCombineThreads, 0, c->stream, r));
+  CK(mpc_launch_pdl(k_renorm, dim3(c->combine_grid), dim3(kCombineThreads), 0, c->stream, r));
   return MPC_OK;
 }
 
@@ -577,6 +522,7 @@ int mpc_ctx_destroy(mpc_ctx* c) {
   if (!c) return MPC_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  mpc_batch_free(c);
   free_all(c);
   for (auto& v : c->ev)
     for (auto& pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
@@ -687,7 +633,7 @@ int mpc_profile_enable(mpc_ctx* c, int on) {
 }
 
 int mpc_profile_read(mpc_ctx* c, int kind, double* total_ms, long long* launches) {
-  if (!c || kind < 0 || kind > 2 || !total_ms || !launches)
+  if (!c || kind < 0 || kind > 3 || !total_ms || !launches)
     return fail(MPC_ERR_ARG, "bad argument");
   CK(cudaSetDevice(c->device));
   CK(cudaStreamSynchronize(c->stream));

@@ -29,21 +29,10 @@
 
 #include "dev_util.cuh"
 #include "plan.h"
+#include "stream_types.h"
 
 namespace mpc {
 
-struct TmapSet {
-  CUtensorMap m[kMaxBlocks];
-};
-
-struct StreamArgs {
-  const double2* y;       // stage input, ntot complex
-  double2* RP;            // row partials
-  double2* CP;            // column partial slots, kStripW complex each
-  const int* cta_slot0;   // first CP slot of each CTA
-  unsigned* status;
-  Geometry g;
-};
 
 __device__ __forceinline__ double2 ld_y(const double2* y, int idx) {
   return __ldg(y + idx);

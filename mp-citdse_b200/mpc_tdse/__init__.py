@@ -92,6 +92,10 @@ def lib():
     L.mpc_sync.argtypes = [C.c_void_p]
     L.mpc_profile_enable.argtypes = [C.c_void_p, C.c_int]
     L.mpc_profile_read.argtypes = [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_longlong)]
+    L.mpc_batch_rhs.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
+    L.mpc_batch_propagate.argtypes = [C.c_void_p, C.c_int, C.POINTER(Pulse), _dp, _dp, C.c_double,
+                                      C.c_double, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
+                                      _dp]
     L.mpc_launch_count.restype = C.c_longlong
     L.mpc_launch_count.argtypes = [C.c_void_p]
     _lib = L
@@ -238,7 +242,36 @@ class Context:
     def sync(self):
         _check(lib().mpc_sync(self._h))
 
-    KERNELS = {"rhs_stream": 0, "combine": 1, "renorm": 2}
+    # -- batched (many pulses) -------------------------------------------
+    def batch_rhs(self, F, X):
+        """dxdt for B states X [B, size] (complex) at fields F [B]."""
+        X = np.ascontiguousarray(X, dtype=np.complex128)
+        B = X.shape[0]
+        F = np.ascontiguousarray(F, dtype=np.float64)
+        xf = X.view(np.float64).reshape(B, -1).copy()
+        out = np.empty_like(xf)
+        _check(lib().mpc_batch_rhs(self._h, B, _ptr(F), _ptr(xf), _ptr(out)))
+        return out.view(np.complex128).reshape(B, -1)
+
+    def batch_propagate(self, pulses, t0, t_end, X, h0=0.05, dt_max=0.2, rtol=1e-10,
+                        atol=1e-10, max_attempts=0):
+        """Adaptive RKF78 of B pulses at once.  pulses: list of Pulse;
+        t0, t_end: [B]; X: [B, size] complex start states.  Returns
+        (X_final, accepted[B], rejected[B], t_final[B])."""
+        B = len(pulses)
+        arr = (Pulse * B)(*pulses)
+        t0 = np.ascontiguousarray(np.broadcast_to(t0, (B,)), dtype=np.float64)
+        t_end = np.ascontiguousarray(np.broadcast_to(t_end, (B,)), dtype=np.float64)
+        xf = np.ascontiguousarray(X, dtype=np.complex128).view(np.float64).reshape(B, -1).copy()
+        acc = np.zeros(B, dtype=np.int32)
+        rej = np.zeros(B, dtype=np.int32)
+        tf = np.zeros(B)
+        _check(lib().mpc_batch_propagate(self._h, B, arr, _ptr(t0), _ptr(t_end), h0, dt_max, rtol,
+                                         atol, int(max_attempts), _ptr(xf), acc.ctypes.data_as(_ip),
+                                         rej.ctypes.data_as(_ip), _ptr(tf)))
+        return xf.view(np.complex128).reshape(B, -1), acc, rej, tf
+
+    KERNELS = {"rhs_stream": 0, "combine": 1, "renorm": 2, "batch": 3}
 
     def profile(self, on=True):
         _check(lib().mpc_profile_enable(self._h, int(bool(on))))
