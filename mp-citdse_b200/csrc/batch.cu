@@ -36,7 +36,10 @@ using namespace mpc;
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 32, NSTB = 3, BTHREADS = 128;
+constexpr int BM = 64, BN = 64, BK = 32, NSTB = 3, BTHREADS = 256;
+// 8 warps per CTA in a 2 (rows) x 4 (columns) grid; each warp owns 32 rows x
+// 16 real columns = 2 x 2 tiles of m16n8.
+constexpr int WM_TILES = 2, WN_TILES = 2;
 constexpr int LDA_P = BM + 4;   // A stored [k][m] (transposed block), pitch in doubles
 constexpr int LDA_Q = BK + 4;   // A stored [m][k]
 constexpr int LDB = BN + 4;     // B stored [k][n]
@@ -128,7 +131,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   const Geometry& g = a.g;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gq = lane >> 2, tq = lane & 3;
-  const int wm = warp >> 1, wn = warp & 1;
+  const int wm = warp & 1, wn = warp >> 1;
 
   // row tile -> state block L and first local row r0
   int L = 0, rt = blockIdx.x;
@@ -188,11 +191,11 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
     }
   };
 
-  double acc[2][4][4];
+  double acc[WM_TILES][WN_TILES][4];
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < WM_TILES; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < WN_TILES; ++j)
 #pragma unroll
       for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
 
@@ -215,9 +218,9 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
     const double sg = isP ? 1.0 : qsign;
 #pragma unroll
     for (int ks = 0; ks < BK / 8; ++ks) {
-      double af[2][4], bf[4][2];
+      double af[WM_TILES][4], bf[WN_TILES][2];
 #pragma unroll
-      for (int mt = 0; mt < 2; ++mt) {
+      for (int mt = 0; mt < WM_TILES; ++mt) {
         const int m = wm * 32 + mt * 16 + gq;
         const int k = ks * 8 + tq;
         if (isP) {
@@ -233,16 +236,16 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
         }
       }
 #pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        const int n = wn * 32 + nt * 8 + gq;
+      for (int nt = 0; nt < WN_TILES; ++nt) {
+        const int n = wn * 16 + nt * 8 + gq;
         const int k = ks * 8 + tq;
         bf[nt][0] = Bs[k * LDB + n];
         bf[nt][1] = Bs[(k + 4) * LDB + n];
       }
 #pragma unroll
-      for (int mt = 0; mt < 2; ++mt)
+      for (int mt = 0; mt < WM_TILES; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) dmma16x8x8(acc[mt][nt], af[mt], bf[nt]);
+        for (int nt = 0; nt < WN_TILES; ++nt) dmma16x8x8(acc[mt][nt], af[mt], bf[nt]);
     }
   }
   cp_wait<0>();
@@ -254,14 +257,14 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   __shared__ double red_n[2][BN / 2];
   __shared__ double red_e[2][BN / 2];
 #pragma unroll
-  for (int nt = 0; nt < 4; ++nt) {
-    const int q = (c0 + wn * 32 + nt * 8) / 2 + tq;  // pulse column
+  for (int nt = 0; nt < WN_TILES; ++nt) {
+    const int q = (c0 + wn * 16 + nt * 8) / 2 + tq;  // pulse column
     const bool qv = q < a.ncol;
     double nsum = 0.0, emax = 0.0;
     const double F = qv ? a.Fs[s * a.ldc + q] : 0.0;
     const double hq = qv ? a.h[q] : 0.0;
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
+    for (int mt = 0; mt < WM_TILES; ++mt)
 #pragma unroll
       for (int hr = 0; hr < 2; ++hr) {
         const int r = r0 + wm * 32 + mt * 16 + gq + 8 * hr;
@@ -327,7 +330,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
         const double oe = __shfl_xor_sync(0xffffffffu, emax, o);
         emax = (oe != oe) ? oe : fmax(emax, oe);
       }
-      const int col = wn * 16 + nt * 4 + tq;  // pulse slot within the CTA
+      const int col = wn * 8 + nt * 4 + tq;  // pulse slot within the CTA
       if (gq == 0) {
         red_n[wm][col] = nsum;
         red_e[wm][col] = emax;
