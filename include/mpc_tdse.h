@@ -149,6 +149,34 @@ int mpc_batch_propagate(mpc_ctx *ctx, int B, const mpc_pulse *pulses, const doub
                         int max_attempts, double *ct, int *accepted, int *rejected,
                         double *t_final);
 
+/* Objective and gradient (new: the reference has no gradients).
+ *
+ * The field of the fixed-step propagation (mpc_propagate semantics: F frozen
+ * at t+dt per step, renormalisation after every step) is the pulse plus a
+ * piecewise-cubic perturbation dE(t) = sum_k u[k] phi((t - t_k)/g),
+ * t_k = k*T/(K-1), phi the Catmull-Rom (Keys a = -1/2) cubic kernel, zero
+ * outside [0, T].  J = 1 - sum_{eig < 0} |c_i(t_N)|^2 (ionisation yield) for
+ * target < 0, else |c_target(t_N)|^2.
+ *
+ * mpc_objective runs the forward pass from ct0 (host) and keeps a state every
+ * ckpt_every steps (<= 0: 64); mpc_objective_backward then returns dJ/du
+ * (grad_u[K]) and dJ/dF_n per step (dJdF[steps]), either may be NULL, by the
+ * discrete adjoint: each checkpoint segment is recomputed and walked back
+ * through the transposed RKF78 stages (about 3 forward passes in all).
+ * mpc_objective_gradient does both. */
+int mpc_objective(mpc_ctx *ctx, const mpc_pulse *pulse, int K, const double *u, double T,
+                  double t0, double dt, int steps, int target, int ckpt_every, const double *ct0,
+                  double *J);
+int mpc_objective_backward(mpc_ctx *ctx, double *grad_u, double *dJdF);
+int mpc_objective_gradient(mpc_ctx *ctx, const mpc_pulse *pulse, int K, const double *u,
+                           double T, double t0, double dt, int steps, int target, int ckpt_every,
+                           const double *ct0, double *J, double *grad_u, double *dJdF);
+
+/* Measures the FP64 tensor-core (mma.sync .f64) and FP64 FMA throughput of
+ * CUDA device `device` in TFLOP/s: the roofline denominators of the batched
+ * GEMM.  Takes ~50 ms. */
+int mpc_probe_fp64_peak(int device, double *dmma_tflops, double *dfma_tflops);
+
 /* Kernel timing (profiling aid).  While enabled, CUDA events on the
  * context's stream bracket every launch of each kernel kind:
  *   MPC_KERNEL_RHS_STREAM (0)  the dipole-block streaming pass,
@@ -159,7 +187,8 @@ int mpc_batch_propagate(mpc_ctx *ctx, int B, const mpc_pulse *pulses, const doub
 #define MPC_KERNEL_RHS_STREAM 0
 #define MPC_KERNEL_COMBINE 1
 #define MPC_KERNEL_RENORM 2
-#define MPC_KERNEL_BATCH 3   /* every kernel of the batched path */
+#define MPC_KERNEL_BATCH_STAGE 3   /* the batched GEMM + RK epilogue */
+#define MPC_KERNEL_BATCH_OTHER 4   /* batched control, apply, compaction */
 int mpc_profile_enable(mpc_ctx *ctx, int on);
 int mpc_profile_read(mpc_ctx *ctx, int kind, double *total_ms, long long *launches);
 

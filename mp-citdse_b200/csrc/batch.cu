@@ -655,7 +655,7 @@ StageArgs stage_args(mpc_ctx* c, int s, int ncol, double rtol, double atol, bool
 }
 
 int launch_stage(mpc_ctx* c, const StageArgs& a) {
-  ProfScope ps(c, 3);
+  ProfScope ps(c, MPC_KERNEL_BATCH_STAGE);
   const dim3 grid(a.nrowtiles, (2 * a.ncol + BN - 1) / BN);
   CK(mpc_launch_pdl(k_batch_stage, grid, dim3(BTHREADS), BATCH_SMEM, c->stream, a));
   return MPC_OK;
@@ -766,17 +766,17 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
       if ((rc = launch_stage(c, stage_args(c, st, ncol, rtol, atol, false)))) return rc;
     ca.ncol = ncol;
     {
-      ProfScope ps(c, 3);
+      ProfScope ps(c, MPC_KERNEL_BATCH_OTHER);
       CK(mpc_launch_pdl(k_batch_control, dim3(blocks_for(ncol, 128)), dim3(128), 0, c->stream, ca));
     }
     aa.ncol = ncol;
     {
-      ProfScope ps(c, 3);
+      ProfScope ps(c, MPC_KERNEL_BATCH_OTHER);
       CK(mpc_launch_pdl(k_batch_apply, dim3(blocks_for((long long)n * ncol, 256)), dim3(256), 0,
                         c->stream, aa));
     }
     {
-      ProfScope ps(c, 3);
+      ProfScope ps(c, MPC_KERNEL_BATCH_OTHER);
       CK(mpc_launch_pdl(k_batch_clear_retired, dim3(blocks_for(ncol, 128)), dim3(128), 0,
                         c->stream, s.retired, ncol));
     }

@@ -151,6 +151,7 @@ struct RenormArgs {
   int ntot;
   int pop_index;
   int step;
+  int hist_base;           // history index = step - hist_base
   double* pop_hist;        // [steps+1], entry step+1 written
   double* norm_hist;       // [steps]
   unsigned* status;
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(kCombineThreads) k_renorm(const __grid_constan
   __syncthreads();
   const double nrm = nrm_sh;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (a.norm_hist) a.norm_hist[a.step] = nrm;
+    if (a.norm_hist) a.norm_hist[a.step - a.hist_base] = nrm;
     if (!(nrm > 0.0) || !isfinite(nrm)) atomicOr(a.status, ST_NONFINITE);
   }
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(kCombineThreads) k_renorm(const __grid_constan
     const double2 o = make_double2(v.x / nrm, v.y / nrm);
     a.x[i] = o;
     if (i == a.pop_index && a.pop_hist)
-      a.pop_hist[a.step + 1] = dadd(dmul(o.x, o.x), dmul(o.y, o.y));
+      a.pop_hist[a.step - a.hist_base + 1] = dadd(dmul(o.x, o.x), dmul(o.y, o.y));
   }
 }
 

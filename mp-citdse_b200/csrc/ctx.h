@@ -55,7 +55,7 @@ struct mpc_ctx {
 
   // profiling: event pairs per kernel kind, and a launch counter
   bool profiling = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[4];
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[5];
   std::vector<cudaEvent_t> ev_pool;
   long long launches = 0;
 
@@ -66,6 +66,7 @@ struct mpc_ctx {
   std::vector<void*> allocs;
 
   mpc_batch_state* batch = nullptr;  // batched-propagation work space (batch.cu)
+  struct mpc_adjoint_state* adj = nullptr;  // adjoint work space (adjoint.cu)
 };
 
 // Launch with programmatic stream serialization (see mpc_tdse.cu).
@@ -96,3 +97,12 @@ struct ProfScope {
 };
 
 void mpc_batch_free(mpc_ctx* c);
+void mpc_adjoint_free(mpc_ctx* c);
+
+// Launch helpers of the single-pulse path (mpc_tdse.cu), used by adjoint.cu.
+int mpc_launch_stream(mpc_ctx* c, const double2* y);
+int mpc_launch_combine_x(mpc_ctx* c, const double2* x, int stage, int step, double dt,
+                         const double2* y, double2* out, bool final_weights, bool no_sum);
+int mpc_launch_renorm_to(mpc_ctx* c, double2* x_out, const double2* xnew, int step, int pop_index,
+                         double* pop_hist, double* norm_hist, int hist_base);
+int mpc_fill_field_table(mpc_ctx* c, const double* F, int steps);

@@ -209,7 +209,9 @@ bool mpc_pdl_enabled() {
 
 namespace {
 
-int launch_stream(mpc_ctx* c, const double2* y) {
+}  // namespace
+
+int mpc_launch_stream(mpc_ctx* c, const double2* y) {
   c->sargs.y = y;
   ProfScope ps(c, MPC_KERNEL_RHS_STREAM);
   CK(mpc_launch_pdl(k_rhs_stream, dim3(c->stream_grid), dim3(kStreamThreads), kStreamSmem,
@@ -219,10 +221,10 @@ int launch_stream(mpc_ctx* c, const double2* y) {
 
 // stage s: k_s = f(y_s); out = x + sum coef*k.  coefs: the row of the next
 // combination (a_{s+1,*}, or b for s == 12), multiplied by dt.
-int launch_combine(mpc_ctx* c, int stage, int step, double dt, const double2* y, double2* out,
-                   bool final_weights, bool no_sum) {
+int mpc_launch_combine_x(mpc_ctx* c, const double2* x, int stage, int step, double dt,
+                         const double2* y, double2* out, bool final_weights, bool no_sum) {
   CombineArgs a{};
-  a.x = c->d_x;
+  a.x = x;
   a.y = y;
   a.k = c->d_k;
   a.out = out;
@@ -249,6 +251,34 @@ int launch_combine(mpc_ctx* c, int stage, int step, double dt, const double2* y,
   ProfScope ps(c, MPC_KERNEL_COMBINE);
   CK(mpc_launch_pdl(k_stage_combine, dim3(c->combine_grid), dim3(kCombineThreads), 0, c->stream, a));
   return MPC_OK;
+}
+
+int mpc_launch_renorm_to(mpc_ctx* c, double2* x_out, const double2* xnew, int step, int pop_index,
+                         double* pop_hist, double* norm_hist, int hist_base) {
+  RenormArgs r{};
+  r.x = x_out;
+  r.xnew = xnew;
+  r.norm_part = c->d_norm_part;
+  r.nparts = c->combine_grid;
+  r.ntot = c->g.ntot;
+  r.pop_index = pop_index;
+  r.step = step;
+  r.hist_base = hist_base;
+  r.pop_hist = pop_hist;
+  r.norm_hist = norm_hist;
+  r.status = c->d_status;
+  ProfScope ps(c, MPC_KERNEL_RENORM);
+  CK(mpc_launch_pdl(k_renorm, dim3(c->combine_grid), dim3(kCombineThreads), 0, c->stream, r));
+  return MPC_OK;
+}
+
+namespace {
+
+int launch_stream(mpc_ctx* c, const double2* y) { return mpc_launch_stream(c, y); }
+
+int launch_combine(mpc_ctx* c, int stage, int step, double dt, const double2* y, double2* out,
+                   bool final_weights, bool no_sum) {
+  return mpc_launch_combine_x(c, c->d_x, stage, step, dt, y, out, final_weights, no_sum);
 }
 
 int launch_renorm(mpc_ctx* c, int step, int pop_index) {
@@ -365,6 +395,13 @@ int run_steps(mpc_ctx* c, double dt, int steps, int pop_index) {
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
+int mpc_fill_field_table(mpc_ctx* c, const double* F, int steps) {
+  int rc;
+  if ((rc = ensure_hist(c, steps))) return rc;
+  CK(cudaMemcpyAsync(c->d_Ftab, F, sizeof(double) * steps, cudaMemcpyHostToDevice, c->stream));
+  return MPC_OK;
+}
+
 extern "C" {
 
 int mpc_version(void) { return 100; }
@@ -523,6 +560,7 @@ int mpc_ctx_destroy(mpc_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   mpc_batch_free(c);
+  mpc_adjoint_free(c);
   free_all(c);
   for (auto& v : c->ev)
     for (auto& pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
@@ -633,7 +671,7 @@ int mpc_profile_enable(mpc_ctx* c, int on) {
 }
 
 int mpc_profile_read(mpc_ctx* c, int kind, double* total_ms, long long* launches) {
-  if (!c || kind < 0 || kind > 3 || !total_ms || !launches)
+  if (!c || kind < 0 || kind > 4 || !total_ms || !launches)
     return fail(MPC_ERR_ARG, "bad argument");
   CK(cudaSetDevice(c->device));
   CK(cudaStreamSynchronize(c->stream));

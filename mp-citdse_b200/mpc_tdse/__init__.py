@@ -96,6 +96,13 @@ def lib():
     L.mpc_batch_propagate.argtypes = [C.c_void_p, C.c_int, C.POINTER(Pulse), _dp, _dp, C.c_double,
                                       C.c_double, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
                                       _dp]
+    L.mpc_probe_fp64_peak.argtypes = [C.c_int, _dp, _dp]
+    L.mpc_objective.argtypes = [C.c_void_p, C.POINTER(Pulse), C.c_int, _dp, C.c_double, C.c_double,
+                                C.c_double, C.c_int, C.c_int, C.c_int, _dp, _dp]
+    L.mpc_objective_backward.argtypes = [C.c_void_p, _dp, _dp]
+    L.mpc_objective_gradient.argtypes = [C.c_void_p, C.POINTER(Pulse), C.c_int, _dp, C.c_double,
+                                         C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp,
+                                         _dp, _dp, _dp]
     L.mpc_launch_count.restype = C.c_longlong
     L.mpc_launch_count.argtypes = [C.c_void_p]
     _lib = L
@@ -144,6 +151,13 @@ def pulse_setup(shape, gauge, Io_au, w_au, cepd, cycles, tau=0.0):
 
 def field(p, t):
     return lib().mpc_field(C.byref(p), t)
+
+
+def probe_fp64_peak(device=0):
+    """(DMMA, DFMA) FP64 TFLOP/s of the device, measured."""
+    a, b = C.c_double(), C.c_double()
+    _check(lib().mpc_probe_fp64_peak(int(device), C.byref(a), C.byref(b)))
+    return a.value, b.value
 
 
 class Context:
@@ -271,7 +285,30 @@ class Context:
                                          rej.ctypes.data_as(_ip), _ptr(tf)))
         return xf.view(np.complex128).reshape(B, -1), acc, rej, tf
 
-    KERNELS = {"rhs_stream": 0, "combine": 1, "renorm": 2, "batch": 3}
+    # -- objective and adjoint gradient -------------------------------------
+    def objective(self, pulse, u, T, t0, dt, steps, x0, target=-1, ckpt_every=64):
+        """Forward pass; J.  Keeps checkpoints for objective_backward."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        J = C.c_double()
+        _check(lib().mpc_objective(self._h, C.byref(pulse), len(u), _ptr(u), float(T), float(t0),
+                                   float(dt), int(steps), int(target), int(ckpt_every),
+                                   _ptr(_state(x0)), C.byref(J)))
+        self._adj_K, self._adj_steps = len(u), int(steps)
+        return J.value
+
+    def objective_backward(self):
+        """(dJ/du [K], dJ/dF_n [steps]) of the last objective call."""
+        g = np.zeros(self._adj_K)
+        f = np.zeros(self._adj_steps)
+        _check(lib().mpc_objective_backward(self._h, _ptr(g), _ptr(f)))
+        return g, f
+
+    def objective_gradient(self, pulse, u, T, t0, dt, steps, x0, target=-1, ckpt_every=64):
+        J = self.objective(pulse, u, T, t0, dt, steps, x0, target, ckpt_every)
+        g, f = self.objective_backward()
+        return J, g, f
+
+    KERNELS = {"rhs_stream": 0, "combine": 1, "renorm": 2, "batch_stage": 3, "batch_other": 4}
 
     def profile(self, on=True):
         _check(lib().mpc_profile_enable(self._h, int(bool(on))))

@@ -77,6 +77,12 @@ class Oracle:
         L.orc_control_eval.argtypes = [C.c_int, _dp, C.c_double, C.c_double]
         L.orc_tableau.argtypes = [_dp, _dp, _dp, _dp]
         L.orc_use_blas.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_objective_gradient.argtypes = [C.c_int, _ip, _dp, _dp, C.c_char, C.c_int, _dp,
+                                             C.c_int, _dp, C.c_double, C.c_double, C.c_double,
+                                             C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.orc_objective.argtypes = [C.c_int, _ip, _dp, _dp, C.c_char, C.c_int, _dp, C.c_int, _dp,
+                                    C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, _dp,
+                                    _dp]
 
     # -- system helpers -------------------------------------------------
     @staticmethod
@@ -135,6 +141,37 @@ class Oracle:
                                              field_mode, max_attempts, _d(xf), _d(stats))
         return xf.view(np.complex128), {"accepted": int(stats[0]), "rejected": int(stats[1]),
                                         "t": stats[2], "h": stats[3], "rc": rc}
+
+    def objective_gradient(self, n, eig, dip, gauge, field_kind, pars, u, T, t0, dt, steps,
+                           x0, target=-1):
+        """(J, dJ/du [K], dJ/dF_n [steps], x_N) of the fixed-step propagation."""
+        n, eig, dip = self._sys(n, eig, dip)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        x0f = _as_f64(x0)
+        J = C.c_double()
+        g = np.zeros(len(u))
+        fb = np.zeros(steps)
+        xN = np.zeros_like(x0f)
+        kind = FIELD_KINDS[field_kind] if isinstance(field_kind, str) else int(field_kind)
+        rc = self.lib.orc_objective_gradient(len(n) - 1, _i(n), _d(eig), _d(dip), gauge.encode(),
+                                             kind, _d(np.ascontiguousarray(pars, dtype=np.float64)),
+                                             len(u), _d(u), T, t0, dt, steps, target, _d(x0f),
+                                             C.byref(J), _d(g), _d(fb), _d(xN))
+        if rc:
+            raise ValueError(f"orc_objective_gradient rc={rc}")
+        return J.value, g, fb, xN.view(np.complex128)
+
+    def objective(self, n, eig, dip, gauge, field_kind, pars, u, T, t0, dt, steps, x0, target=-1):
+        n, eig, dip = self._sys(n, eig, dip)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        J = C.c_double()
+        kind = FIELD_KINDS[field_kind] if isinstance(field_kind, str) else int(field_kind)
+        rc = self.lib.orc_objective(len(n) - 1, _i(n), _d(eig), _d(dip), gauge.encode(), kind,
+                                    _d(np.ascontiguousarray(pars, dtype=np.float64)), len(u), _d(u),
+                                    T, t0, dt, steps, target, _d(_as_f64(x0)), C.byref(J))
+        if rc:
+            raise ValueError(f"orc_objective rc={rc}")
+        return J.value
 
     def field(self, kind, pars, t):
         pars = np.ascontiguousarray(pars, dtype=np.float64)

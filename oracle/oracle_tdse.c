@@ -524,3 +524,161 @@ int orc_propagate_adaptive(int L_max, const int *n, const double *eig,
   free(w.buf);
   return ret;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Discrete adjoint of the fixed-step propagation (own semantics).           */
+/*                                                                           */
+/* Forward per step n: F_n = base(t_n+dt) + dE(t_n+dt); y_s, k_s = M(F_n) y_s */
+/* (M = -i(H0 + F S) length, -i H0 + F K velocity); z_n = x_n + h sum b_j k_j;*/
+/* x_{n+1} = z_n / ||z_n||.  Objective J(x_N): target < 0 -> ionisation      */
+/* yield 1 - sum_{eig<0} |x_i|^2; else |x_target|^2.                         */
+/* Reverse (real inner product Re<u,v>, M^T = M^dagger = -M):               */
+/*   zbar = (lam - x_{n+1} Re<x_{n+1},lam>) / ||z_n||                        */
+/*   kbar_s = h b_s zbar + sum_{s'>s} h a_{s's} ybar_{s'}  (s = 12..0)       */
+/*   ybar_s = -M kbar_s;  dJ/dF_n += -Re<M1 kbar_s, y_s>,  M1 = dM/dF        */
+/*   lam_n = zbar + sum_s ybar_s                                             */
+/* dJ/du_k = sum_n dJ/dF_n * phi((t_n + dt)/g - k).                          */
+/* ------------------------------------------------------------------------ */
+
+/* M1 v (coupling at unit field), with a zero diagonal. */
+static void coupling(const sys_t *s, const double *v, double *out, double *zero_eig) {
+  sys_t z = *s;
+  z.eig = zero_eig;
+  rhs(&z, 1.0, v, out);
+}
+
+int orc_objective_gradient(int L_max, const int *n, const double *eig, const double *dip,
+                           char gauge, int field_kind, const double *pars, int K,
+                           const double *u, double T, double t0, double dt, int steps,
+                           int target, const double *x0, double *J, double *grad_u,
+                           double *Fbar_out, double *xN) {
+  sys_t s;
+  int rc = sys_init(&s, L_max, n, eig, dip, gauge);
+  if (rc) return rc;
+  rk_init();
+  const int m = 2 * s.ntot;
+  const size_t per = (size_t)m;
+  double *X = (double *)malloc(sizeof(double) * per * (steps + 1));
+  double *Ys = (double *)malloc(sizeof(double) * per * (size_t)steps * NST);
+  double *nrm = (double *)malloc(sizeof(double) * steps);
+  double *Fn = (double *)malloc(sizeof(double) * steps);
+  double *tn = (double *)malloc(sizeof(double) * steps);
+  double *zero = (double *)calloc(s.ntot, sizeof(double));
+  work_t w;
+  if (!X || !Ys || !nrm || !Fn || !tn || !zero || work_alloc(&w, m)) return -10;
+  memcpy(X, x0, sizeof(double) * per);
+  double t = t0;
+  for (int st = 0; st < steps; ++st) {
+    double F = orc_field(field_kind, pars, t + dt);
+    if (K > 0) F += orc_control_eval(K, u, T, t + dt);
+    Fn[st] = F;
+    tn[st] = t + dt;
+    const double *x = X + per * st;
+    double *ys = Ys + per * (size_t)st * NST;
+    /* stages, keeping every stage input */
+    memcpy(ys, x, sizeof(double) * per);
+    rhs(&s, F, ys, w.k[0]);
+    for (int q = 1; q < NST; ++q) {
+      stage_sum(m, x, w.k, RK_A[q], dt, ys + per * q);
+      rhs(&s, F, ys + per * q, w.k[q]);
+    }
+    double *xn = X + per * (st + 1);
+    stage_sum(m, x, w.k, RK_B8, dt, xn);
+    double nr = znrm2(s.ntot, xn);
+    for (int i = 0; i < m; ++i) xn[i] /= nr;
+    nrm[st] = nr;
+    t += dt;
+  }
+  const double *xf = X + per * steps;
+  double *lam = (double *)calloc(per, sizeof(double));
+  double *zb = (double *)malloc(sizeof(double) * per);
+  double *kb = (double *)malloc(sizeof(double) * per);
+  double *yb = (double *)malloc(sizeof(double) * per * NST);
+  double *w1 = (double *)malloc(sizeof(double) * per);
+  double Jv = 0.0;
+  if (target < 0) {
+    double b = 0.0;
+    for (int i = 0; i < s.ntot; ++i)
+      if (eig[i] < 0.0) {
+        b += xf[2 * i] * xf[2 * i] + xf[2 * i + 1] * xf[2 * i + 1];
+        lam[2 * i] = -2.0 * xf[2 * i];
+        lam[2 * i + 1] = -2.0 * xf[2 * i + 1];
+      }
+    Jv = 1.0 - b;
+  } else {
+    Jv = xf[2 * target] * xf[2 * target] + xf[2 * target + 1] * xf[2 * target + 1];
+    lam[2 * target] = 2.0 * xf[2 * target];
+    lam[2 * target + 1] = 2.0 * xf[2 * target + 1];
+  }
+  if (xN) memcpy(xN, xf, sizeof(double) * per);
+  for (int st = steps - 1; st >= 0; --st) {
+    const double *x1 = X + per * (st + 1);
+    const double *ys = Ys + per * (size_t)st * NST;
+    double d = 0.0;
+    for (int i = 0; i < m; ++i) d += x1[i] * lam[i];
+    for (int i = 0; i < m; ++i) zb[i] = (lam[i] - x1[i] * d) / nrm[st];
+    const double F = Fn[st];
+    double fb = 0.0;
+    for (int q = NST - 1; q >= 0; --q) {
+      /* kbar_q = h b_q zbar + sum_{q'>q} h a_{q'q} ybar_{q'} */
+      for (int i = 0; i < m; ++i) kb[i] = (dt * RK_B8[q]) * zb[i];
+      for (int qq = q + 1; qq < NST; ++qq) {
+        const double c = dt * RK_A[qq][q];
+        if (c == 0.0) continue;
+        for (int i = 0; i < m; ++i) kb[i] += c * yb[per * qq + i];
+      }
+      coupling(&s, kb, w1, zero); /* M1 kbar */
+      double *ybq = yb + per * q;
+      for (int i = 0; i < s.ntot; ++i) {
+        const double e = eig[i];
+        const double vr = kb[2 * i], vi = kb[2 * i + 1];
+        const double mr = e * vi + F * w1[2 * i], mi = -e * vr + F * w1[2 * i + 1];
+        ybq[2 * i] = -mr;
+        ybq[2 * i + 1] = -mi;
+        fb -= w1[2 * i] * ys[per * q + 2 * i] + w1[2 * i + 1] * ys[per * q + 2 * i + 1];
+      }
+    }
+    for (int i = 0; i < m; ++i) {
+      double a = zb[i];
+      for (int q = 0; q < NST; ++q) a += yb[per * q + i];
+      lam[i] = a;
+    }
+    if (Fbar_out) Fbar_out[st] = fb;
+    if (grad_u && K > 0) {
+      double wts[4];
+      int k0 = control_weights(K, T, tn[st], wts);
+      for (int j = 0; j < 4; ++j)
+        if (wts[j] != 0.0) grad_u[k0 + j] += fb * wts[j];
+    }
+  }
+  *J = Jv;
+  free(X); free(Ys); free(nrm); free(Fn); free(tn); free(zero); free(w.buf);
+  free(lam); free(zb); free(kb); free(yb); free(w1);
+  return 0;
+}
+
+/* Objective only (same forward as orc_objective_gradient). */
+int orc_objective(int L_max, const int *n, const double *eig, const double *dip, char gauge,
+                  int field_kind, const double *pars, int K, const double *u, double T,
+                  double t0, double dt, int steps, int target, const double *x0, double *J) {
+  sys_t s;
+  int rc = sys_init(&s, L_max, n, eig, dip, gauge);
+  if (rc) return rc;
+  const int m = 2 * s.ntot;
+  double *x = (double *)malloc(sizeof(double) * m);
+  memcpy(x, x0, sizeof(double) * m);
+  rc = orc_propagate(L_max, n, eig, dip, gauge, field_kind, pars, K, u, T, t0, dt, steps, 0, x,
+                     NULL, NULL, NULL);
+  double Jv = 0.0;
+  if (target < 0) {
+    double b = 0.0;
+    for (int i = 0; i < s.ntot; ++i)
+      if (eig[i] < 0.0) b += x[2 * i] * x[2 * i] + x[2 * i + 1] * x[2 * i + 1];
+    Jv = 1.0 - b;
+  } else {
+    Jv = x[2 * target] * x[2 * target] + x[2 * target + 1] * x[2 * target + 1];
+  }
+  *J = Jv;
+  free(x);
+  return rc;
+}

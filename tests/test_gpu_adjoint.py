@@ -1,0 +1,91 @@
+"""Adjoint gradients on the GPU against the CPU oracle's discrete adjoint,
+against central finite differences of the GPU forward (h = 1e-6), and through
+the torch.autograd.Function.
+
+Tolerances: objective vs oracle 1e-12; dJ/dF_n and dJ/du vs the oracle's
+adjoint 1e-9 relative to the largest component; finite differences 1e-6
+relative (their own truncation/rounding error is ~1e-9..1e-8).
+"""
+import numpy as np
+import pytest
+
+import mpc_tdse
+from mpc_tdse.systems import hydrogen_like_1e
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(g, seed=0, n_per_l=30, l_max=3, steps=400, K=48):
+    s = hydrogen_like_1e(n_per_l, l_max, gauge=g, seed=seed)
+    Io, w = mpc_tdse.to_au(2e14, 1.5498)
+    tau = mpc_tdse.period(w, 1)
+    p = mpc_tdse.pulse_setup("sine", g, Io, w, 0.0, 1, tau)
+    rng = np.random.default_rng(seed + 1)
+    u = rng.standard_normal(K) * 0.01 * p.Eo
+    x0 = np.zeros(s.ntot, complex)
+    x0[0] = 1.0
+    return s, p, u, steps * 0.1, x0, steps
+
+
+@pytest.mark.parametrize("g", ["l", "v"])
+@pytest.mark.parametrize("target", [-1, 5])
+def test_adjoint_matches_oracle(oracle, g, target):
+    s, p, u, T, x0, steps = _problem(g)
+    kind = "sineEE" if g == "l" else "sineAA"
+    Jo, go, fbo, _ = oracle.objective_gradient(s.n, s.eig, s.dip, g, kind, p.as_array(), u, T,
+                                               0.0, 0.1, steps, x0, target)
+    with mpc_tdse.Context.from_system(s) as ctx:
+        J, gr, fb = ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0, target, ckpt_every=64)
+    assert abs(J - Jo) < 1e-12
+    assert np.max(np.abs(fb - fbo)) <= 1e-9 * np.max(np.abs(fbo))
+    assert np.max(np.abs(gr - go)) <= 1e-9 * np.max(np.abs(go))
+
+
+def test_adjoint_matches_central_differences():
+    s, p, u, T, x0, steps = _problem("l", seed=3)
+    with mpc_tdse.Context.from_system(s) as ctx:
+        J, gr, _ = ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0, -1)
+        h = 1e-6
+        for k in (0, 7, 23, 40):
+            up, um = u.copy(), u.copy()
+            up[k] += h
+            um[k] -= h
+            fd = (ctx.objective(p, up, T, 0.0, 0.1, steps, x0) -
+                  ctx.objective(p, um, T, 0.0, 0.1, steps, x0)) / (2 * h)
+            assert abs(fd - gr[k]) <= 1e-6 * max(abs(fd), 1e-8 * np.max(np.abs(gr))), (k, fd, gr[k])
+
+
+def test_checkpoint_interval_does_not_change_the_gradient():
+    s, p, u, T, x0, steps = _problem("v", seed=4, steps=301)
+    with mpc_tdse.Context.from_system(s) as ctx:
+        J1, g1, f1 = ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0, -1, ckpt_every=64)
+        J2, g2, f2 = ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0, -1, ckpt_every=7)
+        J3, g3, f3 = ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0, -1, ckpt_every=1000)
+    assert J1 == J2 == J3
+    assert np.array_equal(g1, g2) and np.array_equal(g1, g3)
+
+
+def test_objective_equals_plain_forward():
+    """The objective's forward pass is the fixed-step propagation itself."""
+    s, p, u, T, x0, steps = _problem("l", seed=5)
+    with mpc_tdse.Context.from_system(s) as ctx:
+        J = ctx.objective(p, np.zeros_like(u), T, 0.0, 0.1, steps, x0, target=-1)
+        ct, pop, fld, nrm = ctx.propagate(p, 0.0, 0.1, steps, x0)
+    bound = s.eig < 0
+    assert abs(J - (1.0 - np.sum(np.abs(ct[bound]) ** 2))) < 1e-13
+
+
+def test_torch_autograd_function():
+    import torch
+
+    from mpc_tdse.autograd import ControlProblem, control_objective
+
+    s, p, u, T, x0, steps = _problem("l", seed=6)
+    with mpc_tdse.Context.from_system(s) as ctx:
+        prob = ControlProblem(ctx, p, T, 0.0, 0.1, steps, x0)
+        ut = torch.tensor(u, dtype=torch.float64, requires_grad=True)
+        J = control_objective(ut, prob)
+        (2.0 * J).backward()
+        J2, g2, _ = ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0)
+    assert abs(float(J.detach()) - J2) == 0.0
+    assert np.allclose(ut.grad.numpy(), 2.0 * g2, rtol=0, atol=1e-15 * np.max(np.abs(g2)) + 1e-300)
