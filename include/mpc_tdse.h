@@ -82,6 +82,21 @@ int mpc_ctx_create(int L_max, const int *state_sz, const double *eig, const doub
                    char gauge, int device, mpc_ctx **out);
 int mpc_ctx_destroy(mpc_ctx *ctx);
 
+/* Which kernels run mpc_propagate / mpc_advance:
+ *   MPC_PATH_AUTO (0)      resident when the coupling fits in shared memory,
+ *                          streaming otherwise (default);
+ *   MPC_PATH_STREAMING (1) per-stage kernels streaming the dipole blocks
+ *                          from HBM (any size);
+ *   MPC_PATH_RESIDENT (2)  one persistent cooperative kernel per call, each
+ *                          CTA holding its rows' coupling in shared memory
+ *                          (MPC_ERR_ARG if the system does not fit).
+ * Both give the same results within rounding (tested). */
+#define MPC_PATH_AUTO 0
+#define MPC_PATH_STREAMING 1
+#define MPC_PATH_RESIDENT 2
+int mpc_ctx_set_path(mpc_ctx *ctx, int path);
+int mpc_ctx_get_path(mpc_ctx *ctx);   /* the path mpc_advance will take */
+
 /* Total number of states sum(state_sz). */
 int mpc_ctx_size(const mpc_ctx *ctx);
 
@@ -189,6 +204,7 @@ int mpc_probe_fp64_peak(int device, double *dmma_tflops, double *dfma_tflops);
 #define MPC_KERNEL_RENORM 2
 #define MPC_KERNEL_BATCH_STAGE 3   /* the batched GEMM + RK epilogue */
 #define MPC_KERNEL_BATCH_OTHER 4   /* batched control, apply, compaction */
+#define MPC_KERNEL_RESIDENT 5      /* the resident single-pulse propagation */
 int mpc_profile_enable(mpc_ctx *ctx, int on);
 int mpc_profile_read(mpc_ctx *ctx, int kind, double *total_ms, long long *launches);
 

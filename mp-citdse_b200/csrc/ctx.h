@@ -55,7 +55,7 @@ struct mpc_ctx {
 
   // profiling: event pairs per kernel kind, and a launch counter
   bool profiling = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[5];
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[6];
   std::vector<cudaEvent_t> ev_pool;
   long long launches = 0;
 
@@ -67,6 +67,8 @@ struct mpc_ctx {
 
   mpc_batch_state* batch = nullptr;  // batched-propagation work space (batch.cu)
   struct mpc_adjoint_state* adj = nullptr;  // adjoint work space (adjoint.cu)
+  struct mpc_resident_state* resident = nullptr;  // resident path (resident.cu)
+  int path = 0;  // 0 automatic, 1 streaming, 2 resident (MPC_PATH_*)
 };
 
 // Launch with programmatic stream serialization (see mpc_tdse.cu).
@@ -98,6 +100,9 @@ struct ProfScope {
 
 void mpc_batch_free(mpc_ctx* c);
 void mpc_adjoint_free(mpc_ctx* c);
+bool mpc_resident_setup(mpc_ctx* c);
+void mpc_resident_free(mpc_ctx* c);
+int mpc_resident_run(mpc_ctx* c, double dt, int steps, int pop_index);
 
 // Launch helpers of the single-pulse path (mpc_tdse.cu), used by adjoint.cu.
 int mpc_launch_stream(mpc_ctx* c, const double2* y);

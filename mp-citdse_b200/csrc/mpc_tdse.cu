@@ -378,8 +378,14 @@ int fill_fields(mpc_ctx* c, const mpc_pulse* p, double t0, double dt, int steps,
   return MPC_OK;
 }
 
+bool use_resident(mpc_ctx* c) {
+  if (c->path == MPC_PATH_STREAMING) return false;
+  return mpc_resident_setup(c);
+}
+
 int run_steps(mpc_ctx* c, double dt, int steps, int pop_index) {
   int rc;
+  if (steps > 0 && use_resident(c)) return mpc_resident_run(c, dt, steps, pop_index);
   ++c->launches;
   k_pop_init<<<1, 1, 0, c->stream>>>(c->d_x, pop_index, c->d_pop);
   CK(cudaGetLastError());
@@ -561,6 +567,7 @@ int mpc_ctx_destroy(mpc_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   mpc_batch_free(c);
   mpc_adjoint_free(c);
+  mpc_resident_free(c);
   free_all(c);
   for (auto& v : c->ev)
     for (auto& pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
@@ -574,6 +581,21 @@ int mpc_ctx_destroy(mpc_ctx* c) {
 }
 
 int mpc_ctx_size(const mpc_ctx* c) { return c ? c->g.ntot : MPC_ERR_ARG; }
+
+int mpc_ctx_set_path(mpc_ctx* c, int path) {
+  if (!c || path < 0 || path > 2) return fail(MPC_ERR_ARG, "bad path");
+  CK(cudaSetDevice(c->device));
+  if (path == MPC_PATH_RESIDENT && !mpc_resident_setup(c))
+    return fail(MPC_ERR_ARG, "the system's coupling rows do not fit in shared memory");
+  c->path = path;
+  return MPC_OK;
+}
+
+int mpc_ctx_get_path(mpc_ctx* c) {
+  if (!c) return MPC_ERR_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return MPC_ERR_CUDA;
+  return use_resident(c) ? MPC_PATH_RESIDENT : MPC_PATH_STREAMING;
+}
 
 int mpc_ctx_stream(const mpc_ctx* c, void** stream) {
   if (!c || !stream) return fail(MPC_ERR_ARG, "null argument");
@@ -671,7 +693,7 @@ int mpc_profile_enable(mpc_ctx* c, int on) {
 }
 
 int mpc_profile_read(mpc_ctx* c, int kind, double* total_ms, long long* launches) {
-  if (!c || kind < 0 || kind > 4 || !total_ms || !launches)
+  if (!c || kind < 0 || kind > 5 || !total_ms || !launches)
     return fail(MPC_ERR_ARG, "bad argument");
   CK(cudaSetDevice(c->device));
   CK(cudaStreamSynchronize(c->stream));

@@ -97,6 +97,8 @@ def lib():
                                       C.c_double, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
                                       _dp]
     L.mpc_probe_fp64_peak.argtypes = [C.c_int, _dp, _dp]
+    L.mpc_ctx_set_path.argtypes = [C.c_void_p, C.c_int]
+    L.mpc_ctx_get_path.argtypes = [C.c_void_p]
     L.mpc_objective.argtypes = [C.c_void_p, C.POINTER(Pulse), C.c_int, _dp, C.c_double, C.c_double,
                                 C.c_double, C.c_int, C.c_int, C.c_int, _dp, _dp]
     L.mpc_objective_backward.argtypes = [C.c_void_p, _dp, _dp]
@@ -308,7 +310,19 @@ class Context:
         g, f = self.objective_backward()
         return J, g, f
 
-    KERNELS = {"rhs_stream": 0, "combine": 1, "renorm": 2, "batch_stage": 3, "batch_other": 4}
+    KERNELS = {"rhs_stream": 0, "combine": 1, "renorm": 2, "batch_stage": 3, "batch_other": 4,
+               "resident": 5}
+    PATHS = {"auto": 0, "streaming": 1, "resident": 2}
+
+    def set_path(self, path):
+        _check(lib().mpc_ctx_set_path(self._h, self.PATHS.get(path, path)))
+
+    @property
+    def path(self):
+        r = lib().mpc_ctx_get_path(self._h)
+        if r < 0:
+            _check(r)
+        return {1: "streaming", 2: "resident"}[r]
 
     def profile(self, on=True):
         _check(lib().mpc_profile_enable(self._h, int(bool(on))))

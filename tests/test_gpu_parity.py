@@ -70,9 +70,10 @@ def test_rk78_step_matches_oracle(oracle, shape, g):
     assert np.max(np.abs(got - want)) <= 1e-13
 
 
+@pytest.mark.parametrize("path", ["streaming", "resident"])
 @pytest.mark.parametrize("g", ["l", "v"])
-@pytest.mark.parametrize("shape", ["tiny", "ragged", "multistrip", "manyblocks"])
-def test_propagate_matches_oracle(oracle, shape, g):
+@pytest.mark.parametrize("shape", ["tiny", "ragged", "multistrip", "manyblocks", "h1e"])
+def test_propagate_matches_oracle(oracle, shape, g, path):
     s = _sys(shape, g, seed=9)
     x0 = np.zeros(s.ntot, complex)
     x0[0] = 1.0
@@ -82,6 +83,8 @@ def test_propagate_matches_oracle(oracle, shape, g):
     steps = 60
     pop_index = min(3, s.ntot - 1)
     with mpc_tdse.Context.from_system(s) as ctx:
+        ctx.set_path(path)
+        assert ctx.path == path
         ct, pop, fld, nrm = ctx.propagate(p, 0.0, 0.1, steps, x0, pop_index=pop_index)
     kind = "sineEE" if g == "l" else "sineAA"
     cto, popo, fldo, nrmo = oracle.propagate(s.n, s.eig, s.dip, g, kind, p.as_array(), 0.0, 0.1,
@@ -92,8 +95,9 @@ def test_propagate_matches_oracle(oracle, shape, g):
     assert np.max(np.abs(nrm - nrmo)) < 1e-12
 
 
+@pytest.mark.parametrize("path", ["streaming", "resident"])
 @pytest.mark.parametrize("case", [("l", "sine"), ("v", "sine"), ("l", "gaussian")])
-def test_full_pulse_matches_reference_golden(golden, case):
+def test_full_pulse_matches_reference_golden(golden, case, path):
     """A whole 2-cycle pulse (2206 steps) against the reference's propL/propV."""
     g, shape = case
     z = golden("propagate.npz")
@@ -106,6 +110,7 @@ def test_full_pulse_matches_reference_golden(golden, case):
     x0 = np.zeros(int(np.sum(n)), complex)
     x0[0] = 1.0
     with mpc_tdse.Context(n, eig, dip, g) as ctx:
+        ctx.set_path(path)
         ct, pop, fld, nrm = ctx.propagate(p, 0.0, 0.1, steps, x0)
     ref_ct = z[key + "_ct"]
     assert np.max(np.abs(np.abs(ct) ** 2 - np.abs(ref_ct) ** 2)) < 1e-9
@@ -113,12 +118,14 @@ def test_full_pulse_matches_reference_golden(golden, case):
     np.testing.assert_allclose(z[key + "_field"][:, 1], fld, rtol=1e-5, atol=1e-12)
 
 
-def test_repeat_runs_are_bit_identical():
+@pytest.mark.parametrize("path", ["streaming", "resident"])
+def test_repeat_runs_are_bit_identical(path):
     s = _sys("multistrip", "v", seed=2)
     x0 = _x(s.ntot, seed=3)
     Io, w = mpc_tdse.to_au(1e14, 3.179)
     p = mpc_tdse.pulse_setup("sine", "v", Io, w, 0.0, 8, 0.0)
     with mpc_tdse.Context.from_system(s) as ctx:
+        ctx.set_path(path)
         a = ctx.propagate(p, 0.0, 0.1, 25, x0)
         b = ctx.propagate(p, 0.0, 0.1, 25, x0)
     for u, v in zip(a, b):
@@ -133,6 +140,13 @@ def test_unstable_dt_is_rejected():
         with pytest.raises(mpc_tdse.MpcError) as e:
             ctx.propagate(p, 0.0, 1.0, 10, x0)
     assert e.value.code == -5
+
+
+def test_resident_path_is_not_taken_when_the_system_does_not_fit(he2e):
+    with mpc_tdse.Context.from_system(he2e) as ctx:
+        assert ctx.path == "streaming"
+        with pytest.raises(mpc_tdse.MpcError):
+            ctx.set_path("resident")
 
 
 def test_device_resident_advance_equals_propagate():
