@@ -46,9 +46,10 @@ WORKLOADS = {
                  cycles=8, dt=0.1,
                  desc="2e He CI-like, L=0..3, 18000 states, velocity gauge, sin^2 390 nm "
                       "5e14 W/cm^2 8 cycles, dt=0.1, reference semantics"),
-    "h1e": dict(kind="1e", n=(298,) * 6, gauge="l", w_eV=1.5498, Io=1e14, cycles=10, dt=0.1,
-                desc="1e H-like, l=0..5, 298 states/l, length gauge, sin^2 800 nm 1e14 W/cm^2 "
-                     "10 cycles, dt=0.1, reference semantics"),
+    "h1e": dict(kind="1e", n=(292,) * 6, gauge="l", w_eV=1.5498, Io=1e14, cycles=10, dt=0.1,
+                desc="1e hydrogen (Z=1, R=200, 300 B-splines of order 9, linear knots; the "
+                     "292 states/l below 20 a.u.), l=0..5, length gauge, sin^2 800 nm "
+                     "1e14 W/cm^2 10 cycles, dt=0.1, reference semantics"),
 }
 
 
@@ -62,11 +63,13 @@ def load_peaks():
 
 
 def make_system(w):
-    from mpc_tdse.systems import helium_like_2e, hydrogen_like_1e
+    from mpc_tdse.structure1e import hydrogen
+    from mpc_tdse.systems import helium_like_2e
 
     if w["kind"] == "2e":
         return helium_like_2e(w["n"], gauge=w["gauge"], seed=0)
-    return hydrogen_like_1e(w["n"][0], len(w["n"]) - 1, gauge=w["gauge"], seed=0)
+    return hydrogen(n=300, k=9, R=200.0, l_max=len(w["n"]) - 1, gauge=w["gauge"],
+                    states=list(w["n"]))
 
 
 class ClockSampler:
@@ -149,9 +152,9 @@ def measure_batched(local, stream_cls):
     import numpy as np
 
     import mpc_tdse
-    from mpc_tdse.systems import hydrogen_like_1e
+    from mpc_tdse.structure1e import hydrogen
 
-    s = hydrogen_like_1e(298, 5, gauge="l", seed=0)
+    s = hydrogen(n=300, k=9, R=200.0, l_max=5, gauge="l", states=[292] * 6)
     S = int((s.n[:-1].astype(np.int64) * s.n[1:]).sum())
     ctx = mpc_tdse.Context.from_system(s, device=local)
     pulses, taus = batched_pulses(mpc_tdse)
@@ -188,7 +191,8 @@ def measure_batched(local, stream_cls):
     ctx.close()
     value = float(acc.sum()) / sec
     return {
-        "workload": "256 seeded pulses on 1e H-like, l=0..5, 298 states/l (1788), length gauge; "
+        "workload": "256 seeded pulses on 1e hydrogen (300 B-splines, R=200; 292 states/l below "
+                    "20 a.u., l=0..5: 1752 states), length gauge; "
                     "I log-uniform 1e13-5e14 W/cm^2, 400-1600 nm, CEP in [0,2pi), 4-20 cycles; "
                     "adaptive RKF78 rtol=atol=1e-10, dt_max=0.2",
         "value": value, "unit": UNIT, "pulses": B, "accepted_steps": int(acc.sum()),
@@ -217,23 +221,24 @@ def measure_adjoint(local, stream_cls, n_fd=2):
     import numpy as np
 
     import mpc_tdse
-    from mpc_tdse.systems import hydrogen_like_1e
+    from mpc_tdse.structure1e import hydrogen
 
-    s = hydrogen_like_1e(398, 8, gauge="l", seed=0)
+    s = hydrogen(n=400, k=9, R=200.0, l_max=8, gauge="l", states=[388] * 9)
     ctx = mpc_tdse.Context.from_system(s, device=local)
     Io, w = mpc_tdse.to_au(1e14, 1.5498)
     tau = mpc_tdse.period(w, 10)
     p = mpc_tdse.pulse_setup("sine", "l", Io, w, 0.0, 10, tau)
-    steps = int(tau / 0.1)
+    dt = 0.05
+    steps = int(tau / dt)
     rng = np.random.default_rng(1)
     K = 4096
     u = rng.standard_normal(K) * 0.01 * p.Eo
     x0 = np.zeros(s.ntot, complex)
     x0[0] = 1.0
     # warm-up (allocations, module load)
-    ctx.objective_gradient(p, u, tau, 0.0, 0.1, 64, x0)
+    ctx.objective_gradient(p, u, tau, 0.0, dt, 64, x0)
     t0 = time.perf_counter()
-    J = ctx.objective(p, u, tau, 0.0, 0.1, steps, x0)
+    J = ctx.objective(p, u, tau, 0.0, dt, steps, x0)
     t1 = time.perf_counter()
     g, fbar = ctx.objective_backward()
     t2 = time.perf_counter()
@@ -244,15 +249,17 @@ def measure_adjoint(local, stream_cls, n_fd=2):
         up, um = u.copy(), u.copy()
         up[k] += h
         um[k] -= h
-        d = (ctx.objective(p, up, tau, 0.0, 0.1, steps, x0) -
-             ctx.objective(p, um, tau, 0.0, 0.1, steps, x0)) / (2 * h)
+        d = (ctx.objective(p, up, tau, 0.0, dt, steps, x0) -
+             ctx.objective(p, um, tau, 0.0, dt, steps, x0)) / (2 * h)
         fd.append({"k": int(k), "adjoint": float(g[k]), "central_fd": float(d),
                    "rel_err": float(abs(d - g[k]) / max(abs(d), 1e-300))})
     ctx.close()
     return {
-        "workload": "1e H-like, 398 states/l, l=0..8 (3582), length gauge, sin^2 800 nm "
-                    "1e14 W/cm^2 10 cycles, dt=0.1 (%d steps); 4096 piecewise-cubic E(t) "
-                    "controls (sigma = 1%% E0), objective: ionisation yield, checkpoint 64" % steps,
+        "workload": "1e hydrogen (400 B-splines, R=200; 388 states/l below 20 a.u., l=0..8: "
+                    "3492 states), length gauge, sin^2 800 nm 1e14 W/cm^2 10 cycles, dt=0.05 "
+                    "(%d steps, inside the RKF78 stability interval with the field coupling); "
+                    "4096 piecewise-cubic E(t) controls (sigma = 1%% E0), objective: "
+                    "ionisation yield, checkpoint 64" % steps,
         "value": 1.0 / (fwd + bwd), "unit": "gradients/s", "objective": J,
         "forward_s": fwd, "gradient_s": fwd + bwd, "cost_vs_forward": (fwd + bwd) / fwd,
         "forward_pulse_steps_per_s": steps / fwd, "grad_norm": float(np.linalg.norm(g)),
