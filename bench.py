@@ -168,7 +168,7 @@ def measure_batched(local, stream_cls):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ctx.profile(True)
     e0.record(st)
-    X, acc, rej, tf = ctx.batch_propagate(pulses, 0.0, taus, X0, h0=0.05, dt_max=0.2,
+    X, acc, rej, tf = ctx.batch_propagate(pulses, 0.0, taus, X0, h0=0.05, dt_max=0.15,
                                           rtol=1e-10, atol=1e-10)
     e1.record(st)
     ctx.sync()
@@ -194,7 +194,7 @@ def measure_batched(local, stream_cls):
         "workload": "256 seeded pulses on 1e hydrogen (300 B-splines, R=200; 292 states/l below "
                     "20 a.u., l=0..5: 1752 states), length gauge; "
                     "I log-uniform 1e13-5e14 W/cm^2, 400-1600 nm, CEP in [0,2pi), 4-20 cycles; "
-                    "adaptive RKF78 rtol=atol=1e-10, dt_max=0.2",
+                    "adaptive RKF78 rtol=atol=1e-10, dt_max=0.15 (dt_max*max|E| inside the stability interval)",
         "value": value, "unit": UNIT, "pulses": B, "accepted_steps": int(acc.sum()),
         "rejected_steps": int(rej.sum()), "seconds": sec,
         "steps_per_pulse": [int(acc.min()), int(acc.max())],

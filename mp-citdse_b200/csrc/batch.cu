@@ -36,17 +36,26 @@ using namespace mpc;
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 32, NSTB = 3, BTHREADS = 256;
-// 8 warps per CTA in a 2 (rows) x 4 (columns) grid; each warp owns 32 rows x
-// 16 real columns = 2 x 2 tiles of m16n8.
-constexpr int WM_TILES = 2, WN_TILES = 2;
+constexpr int BM = 64, BK = 32, BTHREADS = 256;
 constexpr int LDA_P = BM + 4;   // A stored [k][m] (transposed block), pitch in doubles
 constexpr int LDA_Q = BK + 4;   // A stored [m][k]
-constexpr int LDB = BN + 4;     // B stored [k][n]
 constexpr int A_STAGE = (BK * LDA_P > BM * LDA_Q) ? BK * LDA_P : BM * LDA_Q;
-constexpr int B_STAGE = BK * LDB;
-constexpr int BATCH_SMEM = NSTB * (A_STAGE + B_STAGE) * 8;
 constexpr int kColAlign = 32;   // pulse columns are allocated in multiples of this
+
+// Column-tile shapes (real columns = 2 x pulses).  8 warps in a WGM x WGN
+// grid, each owning WMT x WNT tiles of m16n8; BM = WGM*WMT*16 = 64 rows.
+// The narrowest tile covering the active pulses is used, so that a batch
+// whose pulses have mostly retired does not pay for empty columns.
+template <int BN_> struct Tile;
+template <> struct Tile<64> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 2; };
+template <> struct Tile<32> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 1; };
+template <> struct Tile<16> { static constexpr int WGM = 4, WGN = 2, WMT = 1, WNT = 1; };
+template <int BN_> constexpr int b_stage() { return BK * (BN_ + 4); }
+// NST_ cp.async stages: 3 for the wide tile (two CTAs per SM), 6 for the
+// narrow ones (small grids: more loads in flight per CTA instead)
+template <int BN_, int NST_> constexpr int batch_smem() {
+  return NST_ * (A_STAGE + b_stage<BN_>()) * 8;
+}
 
 __constant__ double c_A[13][13];
 __constant__ double c_B8[13];
@@ -125,13 +134,20 @@ struct StageArgs {
   Geometry g;
 };
 
+template <int BN, int NSTB>
 __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_constant__ StageArgs a) {
   extern __shared__ __align__(16) double bsm[];
+  constexpr int WGM = Tile<BN>::WGM, WMT = Tile<BN>::WMT, WNT = Tile<BN>::WNT;
+  constexpr int LDB = BN + 4;
+  constexpr int B_STAGE = b_stage<BN>();
+  constexpr int WM_TILES = WMT, WN_TILES = WNT;
+  static_assert(Tile<BN>::WGM * Tile<BN>::WGN * 32 == BTHREADS, "8 warps");
+  static_assert(WGM * WMT * 16 == BM && Tile<BN>::WGN * WNT * 8 == BN, "tile shape");
   pdl_trigger();
   const Geometry& g = a.g;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gq = lane >> 2, tq = lane & 3;
-  const int wm = warp & 1, wn = warp >> 1;
+  const int wm = warp % WGM, wn = warp / WGM;
 
   // row tile -> state block L and first local row r0
   int L = 0, rt = blockIdx.x;
@@ -221,7 +237,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
       double af[WM_TILES][4], bf[WN_TILES][2];
 #pragma unroll
       for (int mt = 0; mt < WM_TILES; ++mt) {
-        const int m = wm * 32 + mt * 16 + gq;
+        const int m = wm * (WMT * 16) + mt * 16 + gq;
         const int k = ks * 8 + tq;
         if (isP) {
           af[mt][0] = As[k * LDA_P + m];
@@ -237,7 +253,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
       }
 #pragma unroll
       for (int nt = 0; nt < WN_TILES; ++nt) {
-        const int n = wn * 16 + nt * 8 + gq;
+        const int n = wn * (WNT * 8) + nt * 8 + gq;
         const int k = ks * 8 + tq;
         bf[nt][0] = Bs[k * LDB + n];
         bf[nt][1] = Bs[(k + 4) * LDB + n];
@@ -254,11 +270,11 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   const int s = a.stage;
   const long long nld = (long long)g.ntot * a.ldc;  // complex elements per k slab
   const bool last = (s == kNumStages - 1);
-  __shared__ double red_n[2][BN / 2];
-  __shared__ double red_e[2][BN / 2];
+  __shared__ double red_n[WGM][BN / 2];
+  __shared__ double red_e[WGM][BN / 2];
 #pragma unroll
   for (int nt = 0; nt < WN_TILES; ++nt) {
-    const int q = (c0 + wn * 16 + nt * 8) / 2 + tq;  // pulse column
+    const int q = (c0 + wn * (WNT * 8) + nt * 8) / 2 + tq;  // pulse column
     const bool qv = q < a.ncol;
     double nsum = 0.0, emax = 0.0;
     const double F = qv ? a.Fs[s * a.ldc + q] : 0.0;
@@ -267,7 +283,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
     for (int mt = 0; mt < WM_TILES; ++mt)
 #pragma unroll
       for (int hr = 0; hr < 2; ++hr) {
-        const int r = r0 + wm * 32 + mt * 16 + gq + 8 * hr;
+        const int r = r0 + wm * (WMT * 16) + mt * 16 + gq + 8 * hr;
         if (!qv || r >= nL) continue;
         const long long i = g.state_off[L] + r;
         const long long idx = i * a.ldc + q;
@@ -330,7 +346,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
         const double oe = __shfl_xor_sync(0xffffffffu, emax, o);
         emax = (oe != oe) ? oe : fmax(emax, oe);
       }
-      const int col = wn * 8 + nt * 4 + tq;  // pulse slot within the CTA
+      const int col = wn * (WNT * 4) + nt * 4 + tq;  // pulse slot within the CTA
       if (gq == 0) {
         red_n[wm][col] = nsum;
         red_e[wm][col] = emax;
@@ -342,9 +358,14 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
     if (threadIdx.x < BN / 2) {
       const int q = c0 / 2 + threadIdx.x;
       if (q < a.ncol) {
-        a.normpart[(long long)blockIdx.x * a.ldc + q] = red_n[0][threadIdx.x] + red_n[1][threadIdx.x];
-        const double e0 = red_e[0][threadIdx.x], e1 = red_e[1][threadIdx.x];
-        const double em = (e0 != e0) ? e0 : ((e1 != e1) ? e1 : fmax(e0, e1));
+        double ns = red_n[0][threadIdx.x], em = red_e[0][threadIdx.x];
+#pragma unroll
+        for (int w = 1; w < WGM; ++w) {
+          ns += red_n[w][threadIdx.x];
+          const double e = red_e[w][threadIdx.x];
+          em = (em != em) ? em : ((e != e) ? e : fmax(em, e));
+        }
+        a.normpart[(long long)blockIdx.x * a.ldc + q] = ns;
         atomicMax(&a.err[q], (unsigned long long)__double_as_longlong(em));
       }
     }
@@ -588,8 +609,12 @@ int ensure_batch(mpc_ctx* c, int B) {
     CK(cudaMemcpyToSymbol(c_B8, B8, sizeof B8));
     CK(cudaMemcpyToSymbol(c_E, E, sizeof E));
     CK(cudaMemcpyToSymbol(c_C, Cn, sizeof Cn));
-    CK(cudaFuncSetAttribute(k_batch_stage, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            BATCH_SMEM));
+    CK(cudaFuncSetAttribute(k_batch_stage<64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            batch_smem<64, 3>()));
+    CK(cudaFuncSetAttribute(k_batch_stage<32, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            batch_smem<32, 6>()));
+    CK(cudaFuncSetAttribute(k_batch_stage<16, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            batch_smem<16, 6>()));
     consts = true;
   }
   const int ldc = (B + kColAlign - 1) / kColAlign * kColAlign;
@@ -656,8 +681,17 @@ StageArgs stage_args(mpc_ctx* c, int s, int ncol, double rtol, double atol, bool
 
 int launch_stage(mpc_ctx* c, const StageArgs& a) {
   ProfScope ps(c, MPC_KERNEL_BATCH_STAGE);
-  const dim3 grid(a.nrowtiles, (2 * a.ncol + BN - 1) / BN);
-  CK(mpc_launch_pdl(k_batch_stage, grid, dim3(BTHREADS), BATCH_SMEM, c->stream, a));
+  const int ncr = 2 * a.ncol;
+  if (ncr <= 16) {
+    CK(mpc_launch_pdl(k_batch_stage<16, 6>, dim3(a.nrowtiles, 1), dim3(BTHREADS),
+                      batch_smem<16, 6>(), c->stream, a));
+  } else if (ncr <= 128) {
+    CK(mpc_launch_pdl(k_batch_stage<32, 6>, dim3(a.nrowtiles, (ncr + 31) / 32), dim3(BTHREADS),
+                      batch_smem<32, 6>(), c->stream, a));
+  } else {
+    CK(mpc_launch_pdl(k_batch_stage<64, 3>, dim3(a.nrowtiles, (ncr + 63) / 64), dim3(BTHREADS),
+                      batch_smem<64, 3>(), c->stream, a));
+  }
   return MPC_OK;
 }
 
@@ -789,8 +823,11 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
       if (!done_h[q]) map_h[act++] = q;
     if (act == 0) break;
     // compact when at least one GEMM column tile (32 pulses) can be dropped
-    const int tiles_now = (2 * ncol + BN - 1) / BN, tiles_new = (2 * act + BN - 1) / BN;
-    if (tiles_new < tiles_now) {
+    // compact when the GEMM can drop a column tile or use a narrower one
+    auto width = [](int nc) {
+      return 2 * nc <= 16 ? 16 : (2 * nc <= 128 ? (2 * nc + 31) / 32 * 32 : (2 * nc + 63) / 64 * 64);
+    };
+    if (width(act) < width(ncol)) {
       CK(cudaMemcpyAsync(b->map, map_h.data(), sizeof(int) * act, cudaMemcpyHostToDevice,
                          c->stream));
       const int gb = blocks_for((long long)n * act, 256);
