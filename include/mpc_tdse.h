@@ -187,6 +187,18 @@ int mpc_objective_gradient(mpc_ctx *ctx, const mpc_pulse *pulse, int K, const do
                            double T, double t0, double dt, int steps, int target, int ckpt_every,
                            const double *ct0, double *J, double *grad_u, double *dJdF);
 
+/* Photoelectron spectrum and populations of the context's current state
+ * (after mpc_propagate / mpc_advance), or of ct (host, 2*size doubles) when
+ * non-NULL: pes::genPES1e / genPES2e (src/pes/pes.cpp:48-262) without their
+ * text round trip.  electrons 1: spectrum of each block l binned onto the
+ * l = 1 energies (grid slot k holds bin k, 1 <= k <= state_sz[0]-2);
+ * electrons 2: per-state densities at E_i - threshold (threshold = the
+ * lowest 1e energy of l = 0, as the reference reads it), slot i of block L.
+ * pes: host [(L_max+1) x ngrid], ngrid >= the largest block; stats: host
+ * [4] = ground-state population, norm, yield, excited population (2e). */
+int mpc_pes(mpc_ctx *ctx, int electrons, double threshold, const double *ct, double *pes,
+            int ngrid, double *stats);
+
 /* Measures the FP64 tensor-core (mma.sync .f64) and FP64 FMA throughput of
  * CUDA device `device` in TFLOP/s: the roofline denominators of the batched
  * GEMM.  Takes ~50 ms. */

@@ -97,6 +97,7 @@ def lib():
                                       C.c_double, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
                                       _dp]
     L.mpc_probe_fp64_peak.argtypes = [C.c_int, _dp, _dp]
+    L.mpc_pes.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp, C.c_int, _dp]
     L.mpc_ctx_set_path.argtypes = [C.c_void_p, C.c_int]
     L.mpc_ctx_get_path.argtypes = [C.c_void_p]
     L.mpc_objective.argtypes = [C.c_void_p, C.POINTER(Pulse), C.c_int, _dp, C.c_double, C.c_double,
@@ -286,6 +287,18 @@ class Context:
                                          atol, int(max_attempts), _ptr(xf), acc.ctypes.data_as(_ip),
                                          rej.ctypes.data_as(_ip), _ptr(tf)))
         return xf.view(np.complex128).reshape(B, -1), acc, rej, tf
+
+    # -- photoelectron spectrum ---------------------------------------------
+    def pes(self, electrons=1, threshold=0.0, ct=None):
+        """(pes [(L_max+1) x ngrid], {ground, norm, yield, excited}) of the
+        current state (or of ct)."""
+        ngrid = int(self.n.max())
+        out = np.zeros((len(self.n), ngrid))
+        st = np.zeros(4)
+        cf = None if ct is None else _state(ct)
+        _check(lib().mpc_pes(self._h, int(electrons), float(threshold), _ptr(cf), _ptr(out), ngrid,
+                             _ptr(st)))
+        return out, {"ground": st[0], "norm": st[1], "yield": st[2], "excited": st[3]}
 
     # -- objective and adjoint gradient -------------------------------------
     def objective(self, pulse, u, T, t0, dt, steps, x0, target=-1, ckpt_every=64):

@@ -284,3 +284,39 @@ class Reference:
         if rc:
             raise ValueError(f"ref_propagate rc={rc}")
         return xf.view(np.complex128)
+
+
+def pes_reference(n, eig, ct, electrons=1, threshold=0.0):
+    """pes::genPES1e / genPES2e (src/pes/pes.cpp:48-262) restated with the
+    same loops and first-match bins, on full-precision coefficients.
+    Returns (pes [(L_max+1) x max(n)], ground, norm, yield, excited)."""
+    n = [int(v) for v in n]
+    offs = np.concatenate([[0], np.cumsum(n)])
+    c2 = np.abs(np.asarray(ct)) ** 2
+    ngrid = max(n)
+    pes = np.zeros((len(n), ngrid))
+    ion_yield = 0.0
+    exc = 0.0
+    if electrons == 1:
+        E1 = eig[offs[1]:offs[2]]
+        for l in range(len(n)):
+            for i in range(1, n[l]):
+                for k in range(1, n[0] - 1):
+                    nd = abs(E1[k] - E1[k - 1])
+                    pd = abs(E1[k + 1] - E1[k])
+                    e = eig[offs[l] + i]
+                    if E1[k] - 0.5 * nd < e < E1[k] + 0.5 * pd:
+                        pes[l, k] += c2[offs[l] + i] * 2.0 / (nd + pd)
+                        ion_yield += (E1[k] > 0) * c2[offs[l] + i]
+                        break
+    else:
+        for L in range(len(n)):
+            o = offs[L]
+            for i in range(1, n[L] - 1):
+                e = eig[o + i]
+                if e - threshold > 0.0:
+                    pes[L, i] = c2[o + i] * 2.0 / (eig[o + i + 1] - eig[o + i - 1])
+                    ion_yield += c2[o + i]
+                if o + i > 0:
+                    exc += c2[o + i]
+    return pes, c2[0], c2.sum(), ion_yield, exc
