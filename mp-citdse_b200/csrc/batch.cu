@@ -47,9 +47,12 @@ constexpr int kColAlign = 32;   // pulse columns are allocated in multiples of t
 // The narrowest tile covering the active pulses is used, so that a batch
 // whose pulses have mostly retired does not pay for empty columns.
 template <int BN_> struct Tile;
-template <> struct Tile<64> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 2; };
-template <> struct Tile<32> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 1; };
-template <> struct Tile<16> { static constexpr int WGM = 4, WGN = 2, WMT = 1, WNT = 1; };
+// KS: independent accumulator sets, rotated by k-step and summed once at the
+// end (fixed order), so a warp with few output tiles is not serialised on one
+// accumulator's chain of dependent mma instructions.
+template <> struct Tile<64> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 2, KS = 1; };
+template <> struct Tile<32> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 1, KS = 2; };
+template <> struct Tile<16> { static constexpr int WGM = 4, WGN = 2, WMT = 1, WNT = 1, KS = 4; };
 template <int BN_> constexpr int b_stage() { return BK * (BN_ + 4); }
 // NST_ cp.async stages: 3 for the wide tile (two CTAs per SM), 6 for the
 // narrow ones (small grids: more loads in flight per CTA instead)
@@ -172,48 +175,71 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   pdl_wait();
   const double* Yin = reinterpret_cast<const double*>(a.Yin);
 
+  // Each thread's cp.async assignments are fixed for the whole K loop, so
+  // their source pointers and bounds are set up once; a chunk only adds its
+  // k offset.
+  constexpr int A_PER = BK * (BM / 2) / BTHREADS;       // 16-B copies of A per thread
+  constexpr int BPR = BN / 2;                            // 16-B copies per B row
+  constexpr int B_ROWS = BTHREADS / BPR;                 // B rows per pass
+  constexpr int B_PER = (BK + B_ROWS - 1) / B_ROWS;
+  const int tid = threadIdx.x;
+  const int p_mm = 2 * (tid % (BM / 2)), p_kk0 = tid / (BM / 2);   // P: kk = p_kk0 + 8 i
+  const int q_kk = 2 * (tid % (BK / 2)), q_mm0 = tid / (BK / 2);   // Q: mm = q_mm0 + 16 i
+  const int b_nn = 2 * (tid % BPR), b_kk0 = tid / BPR;
+  const bool p_mv = r0 + p_mm < nL;
+  const bool b_nv = c0 + b_nn < ncr;
+  const long long pitchP = hasP ? g.blk[L - 1].pitch : 0;
+  const long long pitchQ = hasQ ? g.blk[L].pitch : 0;
+  const double* p_base = hasP ? a.D + g.blk[L - 1].d_off + r0 + p_mm : a.D;
+  const double* q_base = hasQ ? a.D + g.blk[L].d_off + (long long)(r0 + q_mm0) * pitchQ + q_kk : a.D;
+  const int yrowP = hasP ? g.state_off[L - 1] : 0, yrowQ = hasQ ? g.state_off[L + 1] : 0;
+
   auto load_chunk = [&](int ch, int st) {
     double* As = bsm + st * (A_STAGE + B_STAGE);
     double* Bs = As + A_STAGE;
     const bool isP = ch < nchP;
     const int k0 = (isP ? ch : ch - nchP) * BK;
     const int nK = isP ? KP : KQ;
-    const int yrow0 = isP ? g.state_off[L - 1] : g.state_off[L + 1];
+    const int yrow0 = isP ? yrowP : yrowQ;
     if (isP) {
-      // A = D_{L-1}^T : copy D_{L-1}[k0+kk][r0+mm] into As[kk][mm]
-      const BlockGeom& bb = g.blk[L - 1];
-      for (int e = threadIdx.x; e < BK * (BM / 2); e += BTHREADS) {
-        const int kk = e / (BM / 2), mm = 2 * (e % (BM / 2));
-        const bool v = (k0 + kk < nK) && (r0 + mm < nL);
-        const double* src = a.D + bb.d_off + (long long)(v ? k0 + kk : 0) * bb.pitch + (v ? r0 + mm : 0);
-        cp_async16(As + kk * LDA_P + mm, src, v);
+      // A = D_{L-1}^T : D_{L-1}[k0+kk][r0+mm] -> As[kk][mm]
+#pragma unroll
+      for (int i = 0; i < A_PER; ++i) {
+        const int kk = p_kk0 + (BTHREADS / (BM / 2)) * i;
+        const bool v = p_mv && (k0 + kk < nK);
+        cp_async16(As + kk * LDA_P + p_mm, v ? p_base + (long long)(k0 + kk) * pitchP : a.D, v);
       }
     } else {
-      // A = D_L : copy D_L[r0+mm][k0+kk] into As[mm][kk]
-      const BlockGeom& bb = g.blk[L];
-      for (int e = threadIdx.x; e < BM * (BK / 2); e += BTHREADS) {
-        const int mm = e / (BK / 2), kk = 2 * (e % (BK / 2));
-        const bool v = (r0 + mm < nL) && (k0 + kk < nK);
-        const double* src = a.D + bb.d_off + (long long)(v ? r0 + mm : 0) * bb.pitch + (v ? k0 + kk : 0);
-        cp_async16(As + mm * LDA_Q + kk, src, v);
+      // A = D_L : D_L[r0+mm][k0+kk] -> As[mm][kk]
+#pragma unroll
+      for (int i = 0; i < A_PER; ++i) {
+        const int mm = q_mm0 + (BTHREADS / (BK / 2)) * i;
+        const bool v = (r0 + mm < nL) && (k0 + q_kk < nK);
+        cp_async16(As + mm * LDA_Q + q_kk,
+                   v ? q_base + (long long)((BTHREADS / (BK / 2)) * i) * pitchQ + k0 : a.D, v);
       }
     }
     // B = Y rows of the coupled block: Bs[kk][nn]
-    for (int e = threadIdx.x; e < BK * (BN / 2); e += BTHREADS) {
-      const int kk = e / (BN / 2), nn = 2 * (e % (BN / 2));
-      const bool v = (k0 + kk < nK) && (c0 + nn < ncr);
-      const double* src = Yin + (long long)(v ? yrow0 + k0 + kk : 0) * ldr + (v ? c0 + nn : 0);
-      cp_async16(Bs + kk * LDB + nn, src, v);
+#pragma unroll
+    for (int i = 0; i < B_PER; ++i) {
+      const int kk = b_kk0 + B_ROWS * i;
+      if (kk < BK) {
+        const bool v = b_nv && (k0 + kk < nK);
+        cp_async16(Bs + kk * LDB + b_nn, v ? Yin + (long long)(yrow0 + k0 + kk) * ldr + c0 + b_nn : Yin, v);
+      }
     }
   };
 
-  double acc[WM_TILES][WN_TILES][4];
+  constexpr int KS = Tile<BN>::KS;
+  double acc_k[KS][WM_TILES][WN_TILES][4];
 #pragma unroll
-  for (int i = 0; i < WM_TILES; ++i)
+  for (int q = 0; q < KS; ++q)
 #pragma unroll
-    for (int j = 0; j < WN_TILES; ++j)
+    for (int i = 0; i < WM_TILES; ++i)
 #pragma unroll
-      for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+      for (int j = 0; j < WN_TILES; ++j)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc_k[q][i][j][v] = 0.0;
 
   for (int p = 0; p < NSTB - 1; ++p) {
     if (p < nch) load_chunk(p, p);
@@ -261,10 +287,22 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
 #pragma unroll
       for (int mt = 0; mt < WM_TILES; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < WN_TILES; ++nt) dmma16x8x8(acc[mt][nt], af[mt], bf[nt]);
+        for (int nt = 0; nt < WN_TILES; ++nt) dmma16x8x8(acc_k[ks % KS][mt][nt], af[mt], bf[nt]);
     }
   }
   cp_wait<0>();
+  double acc[WM_TILES][WN_TILES][4];
+#pragma unroll
+  for (int i = 0; i < WM_TILES; ++i)
+#pragma unroll
+    for (int j = 0; j < WN_TILES; ++j)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        double t = acc_k[0][i][j][v];
+#pragma unroll
+        for (int q = 1; q < KS; ++q) t += acc_k[q][i][j][v];
+        acc[i][j][v] = t;
+      }
 
   // ---------------- fused RK epilogue ----------------
   const int s = a.stage;
@@ -411,11 +449,12 @@ struct ControlArgs {
   int max_attempts;
 };
 
-__device__ void prepare_attempt(const ControlArgs& a, int q) {
+// The next attempt's step: h capped at the time left (the final step lands
+// exactly on t_end).
+__device__ void prepare_step(const ControlArgs& a, int q) {
   const ColState& c = a.c;
   if (c.done[q]) {
     c.hatt[q] = 0.0;
-    for (int s = 0; s < kNumStages; ++s) a.Fs[s * a.ldc + q] = 0.0;
     return;
   }
   double h = c.h[q];
@@ -427,8 +466,6 @@ __device__ void prepare_attempt(const ControlArgs& a, int q) {
   }
   c.hatt[q] = h;
   c.last[q] = last;
-  const mpc_pulse p = c.pulse[q];
-  for (int s = 0; s < kNumStages; ++s) a.Fs[s * a.ldc + q] = dev_field(p, c.t[q] + c_C[s] * h);
 }
 
 __device__ void retire(const ControlArgs& a, int q) {
@@ -441,60 +478,73 @@ __device__ void retire(const ControlArgs& a, int q) {
   c.retired[q] = 1;
 }
 
+// Per pulse: 16 threads.  Thread 0 accepts or rejects the last attempt and
+// sets the next step; then threads 0..12 evaluate the 13 stage fields
+// F(t + c_s h) in parallel.
+constexpr int kCtlLanes = 16;
+
 __global__ void k_batch_control(const __grid_constant__ ControlArgs a) {
   pdl_trigger();
   pdl_wait();
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= a.ncol) return;
+  const int q = (blockIdx.x * blockDim.x + threadIdx.x) / kCtlLanes;
+  const int lane = threadIdx.x % kCtlLanes;
   const ColState& c = a.c;
-  if (a.mode == 0) {
-    c.h[q] = a.h0;
-    c.done[q] = (c.t[q] >= c.t_end[q]) ? 1 : 0;
-    c.accepted[q] = 0;
-    c.retired[q] = 0;
-    a.err[q] = 0ull;
-    if (c.done[q]) retire(a, q);
-    prepare_attempt(a, q);
-    return;
+  if (q < a.ncol && lane == 0) {
+    if (a.mode == 0) {
+      c.h[q] = a.h0;
+      c.done[q] = (c.t[q] >= c.t_end[q]) ? 1 : 0;
+      c.accepted[q] = 0;
+      c.retired[q] = 0;
+      a.err[q] = 0ull;
+      if (c.done[q]) retire(a, q);
+      prepare_step(a, q);
+    } else {
+      c.accepted[q] = 0;
+      if (!c.done[q]) {
+        const double err = __longlong_as_double((long long)a.err[q]);
+        a.err[q] = 0ull;
+        double ns = 0.0;
+        for (int r = 0; r < a.nrowtiles; ++r) ns += a.normpart[(long long)r * a.ldc + q];
+        const double nrm = sqrt(ns);
+        const double hh = c.hatt[q];
+        const double safety = 0.9, facmin = 0.2, facmax = 5.0;
+        double fac;
+        if (err == 0.0) {
+          fac = facmax;
+        } else {
+          fac = safety / sqrt(sqrt(sqrt(err)));
+          fac = fmin(fmax(fac, facmin), facmax);
+        }
+        c.natt[q] += 1;
+        const bool ok = (err <= 1.0) && (nrm > 0.0) && isfinite(nrm);
+        if (ok) {
+          c.t[q] = c.last[q] ? c.t_end[q] : c.t[q] + hh;
+          c.nacc[q] += 1;
+          c.accepted[q] = 1;
+          c.nrm[q] = nrm;
+          double hn = hh * fac;
+          if (hn > a.dt_max) hn = a.dt_max;
+          c.h[q] = hn;
+          if (c.last[q]) c.done[q] = 1;
+        } else {
+          c.nrej[q] += 1;
+          c.h[q] = hh * fmin(fac, 1.0);
+        }
+        // give up after max_attempts, or when rejections have shrunk the step
+        // to nothing (a non-finite error keeps rejecting)
+        if (!c.done[q] && (c.natt[q] >= a.max_attempts ||
+                           c.h[q] < 1e-13 * fmax(1.0, fabs(c.t_end[q]))))
+          c.done[q] = 2;
+        if (c.done[q]) retire(a, q);
+        prepare_step(a, q);
+      }
+    }
   }
-  c.accepted[q] = 0;
-  if (c.done[q]) return;
-  const double err = __longlong_as_double((long long)a.err[q]);
-  a.err[q] = 0ull;
-  double ns = 0.0;
-  for (int r = 0; r < a.nrowtiles; ++r) ns += a.normpart[(long long)r * a.ldc + q];
-  const double nrm = sqrt(ns);
-  const double hh = c.hatt[q];
-  const double safety = 0.9, facmin = 0.2, facmax = 5.0;
-  double fac;
-  if (err == 0.0) {
-    fac = facmax;
-  } else {
-    fac = safety / sqrt(sqrt(sqrt(err)));
-    fac = fmin(fmax(fac, facmin), facmax);
+  __syncthreads();
+  if (q < a.ncol && lane < kNumStages) {
+    const double F = c.done[q] ? 0.0 : dev_field(c.pulse[q], c.t[q] + c_C[lane] * c.hatt[q]);
+    a.Fs[lane * a.ldc + q] = F;
   }
-  c.natt[q] += 1;
-  const bool ok = (err <= 1.0) && (nrm > 0.0) && isfinite(nrm);
-  if (ok) {
-    c.t[q] = c.last[q] ? c.t_end[q] : c.t[q] + hh;
-    c.nacc[q] += 1;
-    c.accepted[q] = 1;
-    c.nrm[q] = nrm;
-    double hn = hh * fac;
-    if (hn > a.dt_max) hn = a.dt_max;
-    c.h[q] = hn;
-    if (c.last[q]) c.done[q] = 1;
-  } else {
-    c.nrej[q] += 1;
-    c.h[q] = hh * fmin(fac, 1.0);
-  }
-  // give up after max_attempts, or when rejections have shrunk the step to
-  // nothing (a non-finite error keeps rejecting)
-  if (!c.done[q] && (c.natt[q] >= a.max_attempts ||
-                     c.h[q] < 1e-13 * fmax(1.0, fabs(c.t_end[q]))))
-    c.done[q] = 2;
-  if (c.done[q]) retire(a, q);
-  prepare_attempt(a, q);
 }
 
 struct ApplyArgs {
@@ -788,7 +838,7 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
   int ncol = B;
   ca.ncol = ncol;
   ca.mode = 0;
-  k_batch_control<<<blocks_for(ncol, 128), 128, 0, c->stream>>>(ca);
+  k_batch_control<<<blocks_for((long long)ncol * kCtlLanes, 128), 128, 0, c->stream>>>(ca);
   CK(cudaGetLastError());
   ca.mode = 1;
 
@@ -801,7 +851,8 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
     ca.ncol = ncol;
     {
       ProfScope ps(c, MPC_KERNEL_BATCH_OTHER);
-      CK(mpc_launch_pdl(k_batch_control, dim3(blocks_for(ncol, 128)), dim3(128), 0, c->stream, ca));
+      CK(mpc_launch_pdl(k_batch_control, dim3(blocks_for((long long)ncol * kCtlLanes, 128)),
+                        dim3(128), 0, c->stream, ca));
     }
     aa.ncol = ncol;
     {
