@@ -27,6 +27,7 @@
 #include <cmath>
 #include <vector>
 
+#include "batch_types.h"
 #include "ctx.h"
 #include "dev_util.cuh"
 #include "plan.h"
@@ -87,33 +88,6 @@ __device__ __forceinline__ void dmma16x8x8(double* c, const double* a, const dou
       "{%0,%1,%2,%3};"
       : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
-}
-
-__device__ double dev_field(const mpc_pulse& p, double t) {
-  const double Eo = p.Eo, w = p.w, cepd = p.cepd, a = p.a, b = p.b;
-  switch (p.kind) {
-    case MPC_FIELD_SINE_EE:
-    case MPC_FIELD_SINE_AA: {
-      const double s = sin(a * t);
-      return (double)(t >= 0.0 && t <= M_PI / a) * Eo * s * s * sin(w * t + cepd);
-    }
-    case MPC_FIELD_SINE_AE: {
-      const double Wt = a * t, s = sin(Wt), wtc = w * t + cepd;
-      return (double)(t >= 0.0 && t <= M_PI / a) * Eo *
-             (w * s * s * cos(wtc) + a * sin(2 * Wt) * sin(wtc));
-    }
-    case MPC_FIELD_SINE_EA: {
-      const double WpP = w + 2.0 * a, WpN = w - 2.0 * a;
-      return (double)(t >= 0.0 && t <= M_PI / a) * 0.5 * Eo *
-             (((1.0 - cos(w * t + cepd)) / w) -
-              0.5 * ((1.0 - cos(WpP * t)) / WpP + (1.0 - cos(WpN * t)) / WpN));
-    }
-    case MPC_FIELD_GAUSS: {
-      const double td = t - 0.5 * b;
-      return (double)(t >= 0.0 && t <= b) * Eo * exp(-td * td / (a * a)) * sin(w * t + cepd);
-    }
-  }
-  return 0.0;
 }
 
 struct StageArgs {
@@ -410,32 +384,6 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   }
 }
 
-// Per-pulse-column state.
-struct ColState {
-  mpc_pulse* pulse;
-  double* t;
-  double* t_end;
-  double* h;       // proposed next step
-  double* hatt;    // step of the current attempt
-  int* last;       // the attempt ends the pulse
-  int* done;
-  int* accepted;   // 1 if the last attempt was accepted
-  int* nacc;
-  int* nrej;
-  int* natt;
-  int* pulse_id;   // column -> pulse index
-  double* nrm;
-  int* retired;    // set when the pulse finishes; cleared once its state is out
-};
-
-// Per-pulse results, indexed by pulse id (columns move; these do not).
-struct PulseResults {
-  int* nacc;
-  int* nrej;
-  double* t;
-  int* status;     // 0 finished at t_end, 2 gave up after max_attempts
-};
-
 struct ControlArgs {
   ColState c;
   PulseResults res;
@@ -731,6 +679,7 @@ StageArgs stage_args(mpc_ctx* c, int s, int ncol, double rtol, double atol, bool
 
 int launch_stage(mpc_ctx* c, const StageArgs& a) {
   ProfScope ps(c, MPC_KERNEL_BATCH_STAGE);
+  ++c->launches;
   const int ncr = 2 * a.ncol;
   if (ncr <= 16) {
     CK(mpc_launch_pdl(k_batch_stage<16, 6>, dim3(a.nrowtiles, 1), dim3(BTHREADS),
@@ -841,11 +790,114 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
   k_batch_control<<<blocks_for((long long)ncol * kCtlLanes, 128), 128, 0, c->stream>>>(ca);
   CK(cudaGetLastError());
   ca.mode = 1;
+  // pulses with nothing to do are retired by the start: write their states out
+  aa.ncol = ncol;
+  k_batch_apply<<<blocks_for((long long)n * ncol, 256), 256, 0, c->stream>>>(aa);
+  k_batch_clear_retired<<<blocks_for(ncol, 128), 128, 0, c->stream>>>(s.retired, ncol);
+  CK(cudaGetLastError());
+  c->launches += 3;
+
+  // Few pulses left on a system whose coupling fits on chip: the persistent
+  // resident kernel takes over (unless the streamed path was asked for).
+  const int pres = (c->path == MPC_PATH_STREAMING) ? 0 : mpc_batch_res_pmax(c);
 
   std::vector<int> done_h(B), map_h(B);
-  std::vector<int> col_ids = ids;  // host mirror of pulse_id per column
+  auto width = [](int nc) {
+    return 2 * nc <= 16 ? 16 : (2 * nc <= 128 ? (2 * nc + 31) / 32 * 32 : (2 * nc + 63) / 64 * 64);
+  };
+  // active columns -> map_h[0 .. act)
+  auto scan = [&](int* act) -> int {
+    CK(cudaMemcpyAsync(done_h.data(), s.done, sizeof(int) * ncol, cudaMemcpyDeviceToHost,
+                       c->stream));
+    unsigned st = 0;
+    CK(cudaMemcpyAsync(&st, c->d_status, sizeof st, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (st) {
+      CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream));
+      return mpc_fail(MPC_ERR_DEVICE, "kernel status 0x%x in the batched propagation", st);
+    }
+    int k = 0;
+    for (int q = 0; q < ncol; ++q)
+      if (!done_h[q]) map_h[k++] = q;
+    *act = k;
+    return MPC_OK;
+  };
+  // Compaction: the active columns move to the front of X and of every
+  // per-column array (the results of retired pulses are already out).
+  auto compact = [&](int act) -> int {
+    CK(cudaMemcpyAsync(b->map, map_h.data(), sizeof(int) * act, cudaMemcpyHostToDevice,
+                       c->stream));
+    const int gb = blocks_for((long long)n * act, 256);
+    k_batch_gather_cols<<<gb, 256, 0, c->stream>>>(b->Y[0], b->X, b->map, n, act, ldc);
+    CK(cudaMemcpyAsync(b->X, b->Y[0], sizeof(double2) * (size_t)n * ldc,
+                       cudaMemcpyDeviceToDevice, c->stream));
+    const int sb = blocks_for(act, 128);
+#define GATHER(field, T)                                                                    \
+  k_gather_scalar<T><<<sb, 128, 0, c->stream>>>(reinterpret_cast<T*>(b->scratch), s.field,  \
+                                               b->map, act);                               \
+  CK(cudaMemcpyAsync(s.field, b->scratch, sizeof(T) * act, cudaMemcpyDeviceToDevice, c->stream));
+    GATHER(pulse, mpc_pulse)
+    GATHER(t, double)
+    GATHER(t_end, double)
+    GATHER(h, double)
+    GATHER(hatt, double)
+    GATHER(last, int)
+    GATHER(done, int)
+    GATHER(accepted, int)
+    GATHER(nacc, int)
+    GATHER(nrej, int)
+    GATHER(natt, int)
+    GATHER(pulse_id, int)
+    GATHER(nrm, double)
+    GATHER(retired, int)
+    for (int st = 0; st < kNumStages; ++st) {
+      k_gather_scalar<double><<<sb, 128, 0, c->stream>>>(reinterpret_cast<double*>(b->scratch),
+                                                         b->Fs + st * ldc, b->map, act);
+      CK(cudaMemcpyAsync(b->Fs + st * ldc, b->scratch, sizeof(double) * act,
+                         cudaMemcpyDeviceToDevice, c->stream));
+    }
+#undef GATHER
+    CK(cudaGetLastError());
+    c->launches += 16;
+    ncol = act;
+    return MPC_OK;
+  };
+
   const int check_every = 8;
   for (long long it = 0;; ++it) {
+    if (it % check_every == 0) {
+      int act = 0;
+      if ((rc = scan(&act))) return rc;
+      if (act == 0) break;
+      if (pres && act <= pres) {
+        if (act < ncol && (rc = compact(act))) return rc;
+        BatchResLaunch l{};
+        l.c = s;
+        l.res = b->res;
+        l.X = b->X;
+        l.XN = b->K;  // k slab 0 (unused by the resident kernel)
+        l.Y0 = b->Y[0];
+        l.Y1 = b->Y[1];
+        l.out = b->out;
+        l.ldc = ldc;
+        l.max_attempts = ca.max_attempts;
+        l.rtol = rtol;
+        l.atol = atol;
+        l.dt_max = dt_max;
+        while (true) {
+          int P = 1;
+          while (P < ncol) P *= 2;
+          l.ncol = ncol;
+          if ((rc = mpc_batch_res_run(c, l, P, P > 1 ? P / 2 + 1 : 0))) return rc;
+          if ((rc = scan(&act))) return rc;
+          if (act == 0) break;
+          if (act < ncol && (rc = compact(act))) return rc;
+        }
+        break;
+      }
+      // compact when the GEMM can drop a column tile or use a narrower one
+      if (width(act) < width(ncol) && (rc = compact(act))) return rc;
+    }
     for (int st = 0; st < kNumStages; ++st)
       if ((rc = launch_stage(c, stage_args(c, st, ncol, rtol, atol, false)))) return rc;
     ca.ncol = ncol;
@@ -865,60 +917,7 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
       CK(mpc_launch_pdl(k_batch_clear_retired, dim3(blocks_for(ncol, 128)), dim3(128), 0,
                         c->stream, s.retired, ncol));
     }
-    if ((it + 1) % check_every) continue;
-    CK(cudaMemcpyAsync(done_h.data(), s.done, sizeof(int) * ncol, cudaMemcpyDeviceToHost,
-                       c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    int act = 0;
-    for (int q = 0; q < ncol; ++q)
-      if (!done_h[q]) map_h[act++] = q;
-    if (act == 0) break;
-    // compact when at least one GEMM column tile (32 pulses) can be dropped
-    // compact when the GEMM can drop a column tile or use a narrower one
-    auto width = [](int nc) {
-      return 2 * nc <= 16 ? 16 : (2 * nc <= 128 ? (2 * nc + 31) / 32 * 32 : (2 * nc + 63) / 64 * 64);
-    };
-    if (width(act) < width(ncol)) {
-      CK(cudaMemcpyAsync(b->map, map_h.data(), sizeof(int) * act, cudaMemcpyHostToDevice,
-                         c->stream));
-      const int gb = blocks_for((long long)n * act, 256);
-      k_batch_gather_cols<<<gb, 256, 0, c->stream>>>(b->Y[0], b->X, b->map, n, act, ldc);
-      CK(cudaMemcpyAsync(b->X, b->Y[0], sizeof(double2) * (size_t)n * ldc,
-                         cudaMemcpyDeviceToDevice, c->stream));
-      const int sb = blocks_for(act, 128);
-#define GATHER(field, T)                                                                    \
-  k_gather_scalar<T><<<sb, 128, 0, c->stream>>>(reinterpret_cast<T*>(b->scratch), s.field,  \
-                                               b->map, act);                               \
-  CK(cudaMemcpyAsync(s.field, b->scratch, sizeof(T) * act, cudaMemcpyDeviceToDevice, c->stream));
-      GATHER(pulse, mpc_pulse)
-      GATHER(t, double)
-      GATHER(t_end, double)
-      GATHER(h, double)
-      GATHER(hatt, double)
-      GATHER(last, int)
-      GATHER(done, int)
-      GATHER(accepted, int)
-      GATHER(nacc, int)
-      GATHER(nrej, int)
-      GATHER(natt, int)
-      GATHER(pulse_id, int)
-      GATHER(nrm, double)
-      GATHER(retired, int)
-      for (int st = 0; st < kNumStages; ++st) {
-        k_gather_scalar<double><<<sb, 128, 0, c->stream>>>(reinterpret_cast<double*>(b->scratch),
-                                                           b->Fs + st * ldc, b->map, act);
-        CK(cudaMemcpyAsync(b->Fs + st * ldc, b->scratch, sizeof(double) * act,
-                           cudaMemcpyDeviceToDevice, c->stream));
-      }
-#undef GATHER
-      CK(cudaGetLastError());
-      // results of pulses retired earlier are already in `out`; keep the host
-      // mirror of the column -> pulse map for the final read-back
-      std::vector<int> nid(act);
-      for (int q = 0; q < act; ++q) nid[q] = col_ids[map_h[q]];
-      col_ids = nid;
-      ncol = act;
-    }
+    c->launches += 3;
   }
   // per-pulse results (indexed by pulse id) and final states
   std::vector<int> na(B), nr(B), stt(B);
@@ -931,7 +930,6 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
   CK(cudaMemcpyAsync(ct, b->out, sizeof(double2) * (size_t)n * B, cudaMemcpyDeviceToHost,
                      c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  (void)col_ids;
   int gave_up = 0;
   for (int i = 0; i < B; ++i) {
     if (accepted) accepted[i] = na[i];

@@ -68,6 +68,7 @@ struct mpc_ctx {
   mpc_batch_state* batch = nullptr;  // batched-propagation work space (batch.cu)
   struct mpc_adjoint_state* adj = nullptr;  // adjoint work space (adjoint.cu)
   struct mpc_resident_state* resident = nullptr;  // resident path (resident.cu)
+  struct mpc_batch_res_state* batch_res = nullptr;  // resident batched path (batch_resident.cu)
   int path = 0;  // 0 automatic, 1 streaming, 2 resident (MPC_PATH_*)
 };
 
@@ -102,6 +103,7 @@ void mpc_batch_free(mpc_ctx* c);
 void mpc_adjoint_free(mpc_ctx* c);
 bool mpc_resident_setup(mpc_ctx* c);
 void mpc_resident_free(mpc_ctx* c);
+void mpc_batch_res_free(mpc_ctx* c);
 int mpc_resident_run(mpc_ctx* c, double dt, int steps, int pop_index);
 
 // Launch helpers of the single-pulse path (mpc_tdse.cu), used by adjoint.cu.

@@ -40,8 +40,9 @@ def _pulses(g, specs):
     return out
 
 
+@pytest.mark.parametrize("path", ["auto", "streaming"])
 @pytest.mark.parametrize("g", ["l", "v"])
-def test_batch_adaptive_matches_oracle(oracle, g):
+def test_batch_adaptive_matches_oracle(oracle, g, path):
     s = hydrogen_like_1e(40, 3, gauge=g, seed=2)
     specs = [(1e14, 1.5498, 1, 0.0), (3e14, 3.0996, 2, 0.3), (5e13, 2.2, 1, 1.1),
              (2e14, 1.8, 2, 2.0), (1e13, 3.5, 1, 0.0)]
@@ -50,6 +51,7 @@ def test_batch_adaptive_matches_oracle(oracle, g):
     X0[:, 0] = 1.0
     kind = "sineEE" if g == "l" else "sineAA"
     with mpc_tdse.Context.from_system(s) as ctx:
+        ctx.set_path(path)
         X, acc, rej, tf = ctx.batch_propagate([p for p, _ in ps], 0.0, [t for _, t in ps], X0,
                                               h0=0.05, dt_max=0.2, rtol=1e-10, atol=1e-10)
     for b, (p, tau) in enumerate(ps):
@@ -61,9 +63,11 @@ def test_batch_adaptive_matches_oracle(oracle, g):
         assert abs(np.linalg.norm(X[b]) - 1.0) < 1e-13
 
 
-def test_batch_uneven_pulses_retire_and_compact(oracle):
+@pytest.mark.parametrize("path", ["auto", "streaming"])
+def test_batch_uneven_pulses_retire_and_compact(oracle, path):
     """70 pulses of 1..6 cycles: columns retire at different times and the
-    batch is compacted repeatedly; every pulse still matches the oracle."""
+    batch is compacted repeatedly (on "auto" the last 8 pulses finish in the
+    persistent resident kernel); every pulse still matches the oracle."""
     s = hydrogen_like_1e(24, 2, gauge="l", seed=4)
     rng = np.random.default_rng(5)
     specs = [(10 ** rng.uniform(13, 14.5), rng.uniform(1.0, 3.5), int(rng.integers(1, 7)),
@@ -72,6 +76,7 @@ def test_batch_uneven_pulses_retire_and_compact(oracle):
     X0 = np.zeros((len(ps), s.ntot), complex)
     X0[:, 0] = 1.0
     with mpc_tdse.Context.from_system(s) as ctx:
+        ctx.set_path(path)
         X, acc, rej, tf = ctx.batch_propagate([p for p, _ in ps], 0.0, [t for _, t in ps], X0,
                                               h0=0.05, dt_max=0.25, rtol=1e-9, atol=1e-9)
     for b in range(0, 70, 7):
@@ -81,3 +86,48 @@ def test_batch_uneven_pulses_retire_and_compact(oracle):
         assert tf[b] == tau
         assert abs(int(acc[b]) - st["accepted"]) <= 1
         assert np.max(np.abs(np.abs(X[b]) ** 2 - np.abs(xo) ** 2)) < 1e-8
+
+
+@pytest.mark.parametrize("B", [1, 5])
+def test_batch_resident_many_rows_per_cta(oracle, B):
+    """A system with more than 16 rows per CTA (several register row groups
+    in the resident kernel) and a velocity-gauge coupling: the persistent
+    resident launch against the oracle's adaptive driver."""
+    s = hydrogen_like_1e(400, 5, gauge="v", seed=7)   # 2400 states: 17 rows on some CTAs
+    specs = [(1e14, 1.5498 + 0.4 * b, 1, 0.2 * b) for b in range(B)]
+    ps = _pulses("v", specs)
+    t_end = [6.0] * B
+    X0 = np.zeros((B, s.ntot), complex)
+    X0[:, 0] = 1.0
+    with mpc_tdse.Context.from_system(s) as ctx:
+        X, acc, rej, tf = ctx.batch_propagate([p for p, _ in ps], 0.0, t_end, X0,
+                                              h0=0.02, dt_max=0.05, rtol=1e-10, atol=1e-10)
+    for b, (p, tau) in enumerate(ps):
+        xo, st = oracle.propagate_adaptive(s.n, s.eig, s.dip, "v", "sineAA", p.as_array(), 0.0,
+                                           t_end[b], 0.02, 0.05, 1e-10, 1e-10, X0[b],
+                                           field_mode=1)
+        assert tf[b] == t_end[b]
+        assert abs(int(acc[b]) - st["accepted"]) <= 1, (b, acc[b], st)
+        assert np.max(np.abs(np.abs(X[b]) ** 2 - np.abs(xo) ** 2)) < 1e-9, b
+
+
+def test_batch_resident_and_streamed_paths_agree():
+    """8 pulses on the 1e hydrogen shapes through both batched paths: same
+    accepted-step counts (within one) and populations within 1e-11."""
+    s = hydrogen_like_1e(298, 5, gauge="l", seed=3)
+    specs = [(10 ** (13 + 0.2 * b), 1.2 + 0.3 * b, 2, 0.4 * b) for b in range(8)]
+    ps = _pulses("l", specs)
+    t_end = [min(tau, 60.0) for _, tau in ps]
+    X0 = np.zeros((8, s.ntot), complex)
+    X0[:, 0] = 1.0
+    out = {}
+    for path in ("auto", "streaming"):
+        with mpc_tdse.Context.from_system(s) as ctx:
+            ctx.set_path(path)
+            out[path] = ctx.batch_propagate([p for p, _ in ps], 0.0, t_end, X0, h0=0.05,
+                                            dt_max=0.1, rtol=1e-10, atol=1e-10)
+    Xa, acca, _, tfa = out["auto"]
+    Xs, accs, _, tfs = out["streaming"]
+    assert np.array_equal(tfa, tfs)
+    assert np.max(np.abs(acca.astype(int) - accs.astype(int))) <= 1
+    assert np.max(np.abs(np.abs(Xa) ** 2 - np.abs(Xs) ** 2)) < 1e-11
