@@ -164,6 +164,17 @@ int mpc_batch_propagate(mpc_ctx *ctx, int B, const mpc_pulse *pulses, const doub
                         int max_attempts, double *ct, int *accepted, int *rejected,
                         double *t_final);
 
+/* Tile autotuner of the batched path (new).  Times each tile variant of the
+ * batched right-hand side GEMM (pulse-column tile width x cp.async pipeline
+ * depth) on this context's system at widths 1, 2, 4, ... up to B pulses and
+ * keeps the fastest per width for the context's later batched calls
+ * (mpc_batch_propagate runs it on first use; every variant sums in the same
+ * order, so the choice never changes results).  If table is non-null it
+ * receives up to cap rows of 4 doubles: pulses, tile width (real columns),
+ * pipeline depth, microseconds per right-hand side of the chosen variant.
+ * Returns the number of rows (>= 0) or an error code. */
+int mpc_batch_autotune(mpc_ctx *ctx, int B, double *table, int cap);
+
 /* Objective and gradient (new: the reference has no gradients).
  *
  * The field of the fixed-step propagation (mpc_propagate semantics: F frozen

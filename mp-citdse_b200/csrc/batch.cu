@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "batch_types.h"
@@ -48,12 +49,12 @@ constexpr int kColAlign = 32;   // pulse columns are allocated in multiples of t
 // The narrowest tile covering the active pulses is used, so that a batch
 // whose pulses have mostly retired does not pay for empty columns.
 template <int BN_> struct Tile;
-// KS: independent accumulator sets, rotated by k-step and summed once at the
-// end (fixed order), so a warp with few output tiles is not serialised on one
-// accumulator's chain of dependent mma instructions.
+// KS: independent accumulator sets rotated by k-step.  Every variant keeps
+// KS = 1 so that all tile shapes sum the coupling in the same order and give
+// bit-identical results: the autotuner's choice never changes the numbers.
 template <> struct Tile<64> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 2, KS = 1; };
-template <> struct Tile<32> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 1, KS = 2; };
-template <> struct Tile<16> { static constexpr int WGM = 4, WGN = 2, WMT = 1, WNT = 1, KS = 4; };
+template <> struct Tile<32> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 1, KS = 1; };
+template <> struct Tile<16> { static constexpr int WGM = 4, WGN = 2, WMT = 1, WNT = 1, KS = 1; };
 template <int BN_> constexpr int b_stage() { return BK * (BN_ + 4); }
 // NST_ cp.async stages: 3 for the wide tile (two CTAs per SM), 6 for the
 // narrow ones (small grids: more loads in flight per CTA instead)
@@ -282,13 +283,18 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   const int s = a.stage;
   const long long nld = (long long)g.ntot * a.ldc;  // complex elements per k slab
   const bool last = (s == kNumStages - 1);
-  __shared__ double red_n[WGM][BN / 2];
+  // norm partials per 16-row m-tile, summed over the tile's rows by a fixed
+  // tree and over the row tile's four m-tiles in order: the same association
+  // for every tile shape
+  __shared__ double red_n[BM / 16][BN / 2];
   __shared__ double red_e[WGM][BN / 2];
 #pragma unroll
   for (int nt = 0; nt < WN_TILES; ++nt) {
     const int q = (c0 + wn * (WNT * 8) + nt * 8) / 2 + tq;  // pulse column
     const bool qv = q < a.ncol;
-    double nsum = 0.0, emax = 0.0;
+    double nsum[WM_TILES], emax = 0.0;
+#pragma unroll
+    for (int mt = 0; mt < WM_TILES; ++mt) nsum[mt] = 0.0;
     const double F = qv ? a.Fs[s * a.ldc + q] : 0.0;
     const double hq = qv ? a.h[q] : 0.0;
 #pragma unroll
@@ -345,22 +351,25 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
           const double ratio = ae / (a.atol + a.rtol * fmax(ax, an));
           emax = fmax(emax, ratio);
           if (!(ratio == ratio)) emax = ratio;  // keep a NaN
-          nsum += o.x * o.x + o.y * o.y;
+          nsum[mt] += o.x * o.x + o.y * o.y;
         }
         a.Yout[idx] = o;
       }
     if (last && !a.want_k_only) {
-      // per pulse: sum over this thread's rows, then over the 8 lanes sharing
-      // tq (fixed xor tree), then over the two warp rows (fixed order)
+      // per pulse and m-tile: this thread's two rows, then the 8 lanes
+      // sharing tq (fixed xor tree)
 #pragma unroll
       for (int o = 4; o < 32; o <<= 1) {
-        nsum += __shfl_xor_sync(0xffffffffu, nsum, o);
+#pragma unroll
+        for (int mt = 0; mt < WM_TILES; ++mt)
+          nsum[mt] += __shfl_xor_sync(0xffffffffu, nsum[mt], o);
         const double oe = __shfl_xor_sync(0xffffffffu, emax, o);
         emax = (oe != oe) ? oe : fmax(emax, oe);
       }
       const int col = wn * (WNT * 4) + nt * 4 + tq;  // pulse slot within the CTA
       if (gq == 0) {
-        red_n[wm][col] = nsum;
+#pragma unroll
+        for (int mt = 0; mt < WM_TILES; ++mt) red_n[wm * WMT + mt][col] = nsum[mt];
         red_e[wm][col] = emax;
       }
     }
@@ -372,8 +381,9 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
       if (q < a.ncol) {
         double ns = red_n[0][threadIdx.x], em = red_e[0][threadIdx.x];
 #pragma unroll
+        for (int m = 1; m < BM / 16; ++m) ns += red_n[m][threadIdx.x];
+#pragma unroll
         for (int w = 1; w < WGM; ++w) {
-          ns += red_n[w][threadIdx.x];
           const double e = red_e[w][threadIdx.x];
           em = (em != em) ? em : ((e != e) ? e : fmax(em, e));
         }
@@ -580,6 +590,9 @@ struct mpc_batch_state {
   ColState c{};
   PulseResults res{};
   std::vector<void*> allocs;
+  // autotuned stage-GEMM variant per width bucket (bucket j: up to 2^j pulses)
+  std::vector<int> tile;
+  std::vector<double> tile_us;
 };
 
 namespace {
@@ -594,8 +607,9 @@ int balloc(mpc_batch_state* b, T** p, size_t count) {
 }
 
 int ensure_batch(mpc_ctx* c, int B) {
-  static bool consts = false;
-  if (!consts) {
+  static bool consts[64] = {};  // per device: constant tables and kernel attributes
+  if (c->device < 0 || c->device >= 64) return mpc_fail(MPC_ERR_ARG, "device %d", c->device);
+  if (!consts[c->device]) {
     double A[13][13], B8[13], E[13], Cn[13];
     for (int i = 0; i < 13; ++i) {
       for (int j = 0; j < 13; ++j) A[i][j] = rkf78::A[i][j];
@@ -607,13 +621,17 @@ int ensure_batch(mpc_ctx* c, int B) {
     CK(cudaMemcpyToSymbol(c_B8, B8, sizeof B8));
     CK(cudaMemcpyToSymbol(c_E, E, sizeof E));
     CK(cudaMemcpyToSymbol(c_C, Cn, sizeof Cn));
-    CK(cudaFuncSetAttribute(k_batch_stage<64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            batch_smem<64, 3>()));
-    CK(cudaFuncSetAttribute(k_batch_stage<32, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            batch_smem<32, 6>()));
+    CK(cudaFuncSetAttribute(k_batch_stage<16, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            batch_smem<16, 3>()));
     CK(cudaFuncSetAttribute(k_batch_stage<16, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             batch_smem<16, 6>()));
-    consts = true;
+    CK(cudaFuncSetAttribute(k_batch_stage<32, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            batch_smem<32, 3>()));
+    CK(cudaFuncSetAttribute(k_batch_stage<32, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            batch_smem<32, 6>()));
+    CK(cudaFuncSetAttribute(k_batch_stage<64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            batch_smem<64, 3>()));
+    consts[c->device] = true;
   }
   const int ldc = (B + kColAlign - 1) / kColAlign * kColAlign;
   if (c->batch && c->batch->ldc >= ldc) return MPC_OK;
@@ -677,20 +695,97 @@ StageArgs stage_args(mpc_ctx* c, int s, int ncol, double rtol, double atol, bool
   return a;
 }
 
+// Stage-GEMM variants: pulse-column tile width (real columns) and cp.async
+// pipeline depth.  Three-stage variants fit two CTAs per SM.
+struct TileVariant {
+  int bn, nst;
+};
+constexpr TileVariant kVariants[] = {{16, 3}, {16, 6}, {32, 3}, {32, 6}, {64, 3}};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+int width_bucket(int ncol) {
+  int j = 0;
+  while ((1 << j) < ncol) ++j;
+  return j;
+}
+
+// Before tuning: the narrowest tile that covers the pulses.
+int default_variant(int ncol) {
+  const int ncr = 2 * ncol;
+  return ncr <= 16 ? 1 : (ncr <= 128 ? 3 : 4);
+}
+
+template <int BN, int NST>
+cudaError_t launch_tile(mpc_ctx* c, const StageArgs& a) {
+  const int ncr = 2 * a.ncol;
+  return mpc_launch_pdl(k_batch_stage<BN, NST>, dim3(a.nrowtiles, (ncr + BN - 1) / BN),
+                        dim3(BTHREADS), batch_smem<BN, NST>(), c->stream, a);
+}
+
+cudaError_t launch_variant(mpc_ctx* c, int v, const StageArgs& a) {
+  switch (v) {
+    case 0: return launch_tile<16, 3>(c, a);
+    case 1: return launch_tile<16, 6>(c, a);
+    case 2: return launch_tile<32, 3>(c, a);
+    case 3: return launch_tile<32, 6>(c, a);
+    default: return launch_tile<64, 3>(c, a);
+  }
+}
+
 int launch_stage(mpc_ctx* c, const StageArgs& a) {
   ProfScope ps(c, MPC_KERNEL_BATCH_STAGE);
   ++c->launches;
-  const int ncr = 2 * a.ncol;
-  if (ncr <= 16) {
-    CK(mpc_launch_pdl(k_batch_stage<16, 6>, dim3(a.nrowtiles, 1), dim3(BTHREADS),
-                      batch_smem<16, 6>(), c->stream, a));
-  } else if (ncr <= 128) {
-    CK(mpc_launch_pdl(k_batch_stage<32, 6>, dim3(a.nrowtiles, (ncr + 31) / 32), dim3(BTHREADS),
-                      batch_smem<32, 6>(), c->stream, a));
-  } else {
-    CK(mpc_launch_pdl(k_batch_stage<64, 3>, dim3(a.nrowtiles, (ncr + 63) / 64), dim3(BTHREADS),
-                      batch_smem<64, 3>(), c->stream, a));
+  const std::vector<int>& t = c->batch->tile;
+  const int j = width_bucket(a.ncol);
+  const int v = j < (int)t.size() ? t[j] : default_variant(a.ncol);
+  CK(launch_variant(c, v, a));
+  return MPC_OK;
+}
+
+// Times every variant on a single right-hand side (stage 0, k only) at
+// widths 1, 2, 4, ... up to max_cols pulses and keeps the fastest per width.
+// Every variant sums in the same order, so the choice affects speed only.
+int autotune(mpc_ctx* c, int max_cols) {
+  mpc_batch_state* b = c->batch;
+  const int top = width_bucket(std::min(std::max(max_cols, 1), b->ldc));
+  std::vector<int> tile(top + 1);
+  std::vector<double> us((size_t)(top + 1) * kNumVariants);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int rc = MPC_OK;
+  for (int j = 0; j <= top && rc == MPC_OK; ++j) {
+    const int w = std::min(1 << j, b->ldc);
+    const StageArgs a = stage_args(c, 0, w, 0.0, 0.0, true);
+    double best = 1e300;
+    for (int v = 0; v < kNumVariants && rc == MPC_OK; ++v) {
+      cudaError_t e = cudaSuccess;
+      for (int r = 0; r < 2 && e == cudaSuccess; ++r) e = launch_variant(c, v, a);
+      if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
+      const int reps = 5;
+      for (int r = 0; r < reps && e == cudaSuccess; ++r) e = launch_variant(c, v, a);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.0f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) {
+        rc = mpc_fail(MPC_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+        break;
+      }
+      c->launches += 2 + reps;
+      const double t = 1000.0 * ms / reps;
+      us[(size_t)j * kNumVariants + v] = t;
+      if (t < best) {
+        best = t;
+        tile[j] = v;
+      }
+    }
   }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  b->tile = tile;
+  b->tile_us = us;
   return MPC_OK;
 }
 
@@ -727,6 +822,24 @@ int mpc_batch_rhs(mpc_ctx* c, int B, const double* F, const double* x, double* d
                      c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return MPC_OK;
+}
+
+int mpc_batch_autotune(mpc_ctx* c, int B, double* table, int cap) {
+  if (!c || B <= 0 || (table && cap < 0)) return mpc_fail(MPC_ERR_ARG, "bad argument");
+  CK(cudaSetDevice(c->device));
+  int rc;
+  if ((rc = ensure_batch(c, B))) return rc;
+  if ((rc = autotune(c, B))) return rc;
+  const mpc_batch_state* b = c->batch;
+  const int rows = (int)b->tile.size();
+  for (int j = 0; table && j < rows && j < cap; ++j) {
+    const int v = b->tile[j];
+    table[4 * j + 0] = std::min(1 << j, b->ldc);
+    table[4 * j + 1] = kVariants[v].bn;
+    table[4 * j + 2] = kVariants[v].nst;
+    table[4 * j + 3] = b->tile_us[(size_t)j * kNumVariants + v];
+  }
+  return rows;
 }
 
 int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0,
@@ -863,50 +976,20 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
     return MPC_OK;
   };
 
-  const int check_every = 8;
-  for (long long it = 0;; ++it) {
-    if (it % check_every == 0) {
-      int act = 0;
-      if ((rc = scan(&act))) return rc;
-      if (act == 0) break;
-      if (pres && act <= pres) {
-        if (act < ncol && (rc = compact(act))) return rc;
-        BatchResLaunch l{};
-        l.c = s;
-        l.res = b->res;
-        l.X = b->X;
-        l.XN = b->K;  // k slab 0 (unused by the resident kernel)
-        l.Y0 = b->Y[0];
-        l.Y1 = b->Y[1];
-        l.out = b->out;
-        l.ldc = ldc;
-        l.max_attempts = ca.max_attempts;
-        l.rtol = rtol;
-        l.atol = atol;
-        l.dt_max = dt_max;
-        while (true) {
-          int P = 1;
-          while (P < ncol) P *= 2;
-          l.ncol = ncol;
-          if ((rc = mpc_batch_res_run(c, l, P, P > 1 ? P / 2 + 1 : 0))) return rc;
-          if ((rc = scan(&act))) return rc;
-          if (act == 0) break;
-          if (act < ncol && (rc = compact(act))) return rc;
-        }
-        break;
-      }
-      // compact when the GEMM can drop a column tile or use a narrower one
-      if (width(act) < width(ncol) && (rc = compact(act))) return rc;
-    }
+  if (b->tile.empty() && !std::getenv("MPC_NO_AUTOTUNE") && (rc = autotune(c, B))) return rc;
+
+  // One attempted step of every active pulse: 13 stage GEMMs, the step
+  // controller, the accepted-state update and the retirement flags.
+  auto launch_attempt = [&]() -> int {
     for (int st = 0; st < kNumStages; ++st)
       if ((rc = launch_stage(c, stage_args(c, st, ncol, rtol, atol, false)))) return rc;
     ca.ncol = ncol;
+    aa.ncol = ncol;
     {
       ProfScope ps(c, MPC_KERNEL_BATCH_OTHER);
       CK(mpc_launch_pdl(k_batch_control, dim3(blocks_for((long long)ncol * kCtlLanes, 128)),
                         dim3(128), 0, c->stream, ca));
     }
-    aa.ncol = ncol;
     {
       ProfScope ps(c, MPC_KERNEL_BATCH_OTHER);
       CK(mpc_launch_pdl(k_batch_apply, dim3(blocks_for((long long)n * ncol, 256)), dim3(256), 0,
@@ -918,7 +1001,86 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
                         c->stream, s.retired, ncol));
     }
     c->launches += 3;
+    return MPC_OK;
+  };
+  // Attempts run in groups of check_every between reads of the done flags;
+  // a group is captured once per active width as a CUDA graph and replayed
+  // (not while profiling, whose per-launch events stay outside graphs).
+  const int check_every = 8;
+  bool use_graph = !c->profiling && !std::getenv("MPC_NO_GRAPH");
+  cudaGraphExec_t gexec = nullptr;
+  int g_ncol = -1;
+  auto drop_graph = [&]() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+    g_ncol = -1;
+  };
+  auto run_group = [&]() -> int {
+    if (use_graph && g_ncol != ncol) {
+      drop_graph();
+      cudaGraph_t graph = nullptr;
+      bool ok = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      const long long l0 = c->launches;
+      int lrc = MPC_OK;
+      for (int k = 0; ok && k < check_every && lrc == MPC_OK; ++k) lrc = launch_attempt();
+      if (ok) ok = cudaStreamEndCapture(c->stream, &graph) == cudaSuccess && lrc == MPC_OK;
+      if (ok) ok = cudaGraphInstantiate(&gexec, graph, 0) == cudaSuccess;
+      if (graph) cudaGraphDestroy(graph);
+      c->launches = l0;
+      if (!ok) {  // capture unavailable: plain launches from here on
+        cudaGetLastError();
+        gexec = nullptr;
+        use_graph = false;
+      } else {
+        g_ncol = ncol;
+      }
+    }
+    if (use_graph) {
+      CK(cudaGraphLaunch(gexec, c->stream));
+      c->launches += 16LL * check_every;
+      return MPC_OK;
+    }
+    for (int k = 0; k < check_every; ++k)
+      if ((rc = launch_attempt())) return rc;
+    return MPC_OK;
+  };
+
+  for (;;) {
+    int act = 0;
+    if ((rc = scan(&act))) break;
+    if (act == 0) break;
+    if (pres && act <= pres) {
+      if (act < ncol && (rc = compact(act))) break;
+      BatchResLaunch l{};
+      l.c = s;
+      l.res = b->res;
+      l.X = b->X;
+      l.XN = b->K;  // k slab 0 (unused by the resident kernel)
+      l.Y0 = b->Y[0];
+      l.Y1 = b->Y[1];
+      l.out = b->out;
+      l.ldc = ldc;
+      l.max_attempts = ca.max_attempts;
+      l.rtol = rtol;
+      l.atol = atol;
+      l.dt_max = dt_max;
+      while (true) {
+        int P = 1;
+        while (P < ncol) P *= 2;
+        l.ncol = ncol;
+        if ((rc = mpc_batch_res_run(c, l, P, P > 1 ? P / 2 + 1 : 0))) break;
+        if ((rc = scan(&act))) break;
+        if (act == 0) break;
+        if (act < ncol && (rc = compact(act))) break;
+      }
+      break;
+    }
+    // compact when the GEMM can drop a column tile or use a narrower one
+    if (width(act) < width(ncol) && (rc = compact(act))) break;
+    if ((rc = run_group())) break;
   }
+  drop_graph();
+  if (rc) return rc;
   // per-pulse results (indexed by pulse id) and final states
   std::vector<int> na(B), nr(B), stt(B);
   std::vector<double> tf(B);

@@ -93,6 +93,7 @@ def lib():
     L.mpc_profile_enable.argtypes = [C.c_void_p, C.c_int]
     L.mpc_profile_read.argtypes = [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_longlong)]
     L.mpc_batch_rhs.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
+    L.mpc_batch_autotune.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]
     L.mpc_batch_propagate.argtypes = [C.c_void_p, C.c_int, C.POINTER(Pulse), _dp, _dp, C.c_double,
                                       C.c_double, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
                                       _dp]
@@ -269,6 +270,15 @@ class Context:
         out = np.empty_like(xf)
         _check(lib().mpc_batch_rhs(self._h, B, _ptr(F), _ptr(xf), _ptr(out)))
         return out.view(np.complex128).reshape(B, -1)
+
+    def batch_autotune(self, B):
+        """Tunes the batched GEMM tiles up to B pulses; returns rows of
+        (pulses, tile width in real columns, pipeline depth, us per RHS)."""
+        cap = 32
+        tab = np.zeros((cap, 4))
+        r = lib().mpc_batch_autotune(self._h, int(B), _ptr(tab), cap)
+        _check(min(r, 0))
+        return [(int(a), int(b), int(c), float(d)) for a, b, c, d in tab[:r]]
 
     def batch_propagate(self, pulses, t0, t_end, X, h0=0.05, dt_max=0.2, rtol=1e-10,
                         atol=1e-10, max_attempts=0):

@@ -131,3 +131,36 @@ def test_batch_resident_and_streamed_paths_agree():
     assert np.array_equal(tfa, tfs)
     assert np.max(np.abs(acca.astype(int) - accs.astype(int))) <= 1
     assert np.max(np.abs(np.abs(Xa) ** 2 - np.abs(Xs) ** 2)) < 1e-11
+
+
+def test_autotune_table_and_variants_bit_identical(monkeypatch):
+    """The autotuner reports one row per width; results do not depend on the
+    tile chosen (every variant sums in the same order) nor on whether the
+    attempt groups run as captured CUDA graphs."""
+    s = hydrogen_like_1e(120, 4, gauge="l", seed=9)
+    rng = np.random.default_rng(3)
+    specs = [(10 ** rng.uniform(13, 14), rng.uniform(1.5, 3.0), 1, rng.uniform(0, 6))
+             for _ in range(40)]
+    ps = _pulses("l", specs)
+    t_end = [min(tau, 20.0) for _, tau in ps]
+    X0 = np.zeros((len(ps), s.ntot), complex)
+    X0[:, 0] = 1.0
+
+    def run(env):
+        for k in ("MPC_NO_AUTOTUNE", "MPC_NO_GRAPH"):
+            monkeypatch.delenv(k, raising=False)
+        for k in env:
+            monkeypatch.setenv(k, "1")
+        with mpc_tdse.Context.from_system(s) as ctx:
+            ctx.set_path("streaming")
+            tab = None if env else ctx.batch_autotune(len(ps))
+            return ctx.batch_propagate([p for p, _ in ps], 0.0, t_end, X0, h0=0.05, dt_max=0.2,
+                                       rtol=1e-10, atol=1e-10), tab
+
+    (Xa, acca, _, _), tab = run([])
+    assert [r[0] for r in tab] == [1, 2, 4, 8, 16, 32, 64]
+    assert all(r[1] in (16, 32, 64) and r[2] in (3, 6) and r[3] > 0 for r in tab)
+    for env in (["MPC_NO_AUTOTUNE"], ["MPC_NO_GRAPH"], ["MPC_NO_AUTOTUNE", "MPC_NO_GRAPH"]):
+        (Xb, accb, _, _), _ = run(env)
+        assert np.array_equal(acca, accb), env
+        assert np.array_equal(Xa, Xb), env
