@@ -181,8 +181,12 @@ int mpc_batch_autotune(mpc_ctx *ctx, int B, double *table, int cap);
  * at t+dt per step, renormalisation after every step) is the pulse plus a
  * piecewise-cubic perturbation dE(t) = sum_k u[k] phi((t - t_k)/g),
  * t_k = k*T/(K-1), phi the Catmull-Rom (Keys a = -1/2) cubic kernel, zero
- * outside [0, T].  J = 1 - sum_{eig < 0} |c_i(t_N)|^2 (ionisation yield) for
- * target < 0, else |c_target(t_N)|^2.
+ * outside [0, T].  J = 1 - sum_{eig < thr} |c_i(t_N)|^2 (the yield above the
+ * threshold thr, 0 unless mpc_objective_threshold set it: ionisation for 1e;
+ * for 2e CI energies measured from the doubly-charged ion, double
+ * ionisation, and thr = -Z^2/2 gives single ionisation) for target < 0, else
+ * |c_target(t_N)|^2.  The final state has unit norm, so the yield is
+ * evaluated as sum_{eig >= thr} |c_i|^2 (no cancellation for small yields).
  *
  * mpc_objective runs the forward pass from ct0 (host) and keeps a state every
  * ckpt_every steps (<= 0: 64); mpc_objective_backward then returns dJ/du
@@ -190,6 +194,7 @@ int mpc_batch_autotune(mpc_ctx *ctx, int B, double *table, int cap);
  * discrete adjoint: each checkpoint segment is recomputed and walked back
  * through the transposed RKF78 stages (about 3 forward passes in all).
  * mpc_objective_gradient does both. */
+int mpc_objective_threshold(mpc_ctx *ctx, double thr);
 int mpc_objective(mpc_ctx *ctx, const mpc_pulse *pulse, int K, const double *u, double T,
                   double t0, double dt, int steps, int target, int ckpt_every, const double *ct0,
                   double *J);

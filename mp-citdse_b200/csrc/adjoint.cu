@@ -7,8 +7,15 @@
 // give z_n = x_n + h sum_j b_j k_j, and x_{n+1} = z_n / ||z_n||.  The control
 // perturbation dE(t) = sum_k u_k phi((t - t_k)/g) is piecewise cubic
 // (Catmull-Rom / Keys a = -1/2 kernel) over K samples on [0, T].
-// Objective J(x_N): ionisation yield 1 - sum_{E_i < 0} |x_i|^2, or the
-// population |x_target|^2.
+// Objective J(x_N): the yield above a threshold, 1 - sum_{E_i < thr} |x_i|^2
+// (thr = 0: ionisation of a 1e system, double ionisation of a 2e system whose
+// energies are given relative to the doubly-charged ion; thr = the ion's
+// ground-state energy: single ionisation), or the population |x_target|^2.
+// Since every step renormalises, ||x_N|| = 1 and the yield is evaluated as
+// sum_{E_i >= thr} |x_i|^2, which keeps small yields (double ionisation,
+// ~1e-6) free of the cancellation in 1 - (1 - J); its seed 2 x on those states
+// differs from -2 x on the others by 2 x_N, which the adjoint of the
+// normalisation removes.
 //
 // Reverse mode.  The generator M(F) = -i(H0 + F S) (length) or -i H0 + F K
 // (velocity) is anti-Hermitian, so for the real inner product Re<u, v> its
@@ -217,9 +224,10 @@ __global__ void k_adj_fbar(const double* fpart, int nblocks, double* fbar_n) {
   if (threadIdx.x == 0) *fbar_n = s;
 }
 
-// lam_N = dJ/dx_N: yield -> -2 x on bound states (E < 0); target -> 2 x_t.
+// lam_N = dJ/dx_N: yield -> 2 x on the states at or above the threshold;
+// target -> 2 x_t.
 __global__ void k_adj_seed(const double2* x, const double* eps, double2* lam, int target,
-                           int ntot) {
+                           double thr, int ntot) {
   pdl_trigger();
   pdl_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -227,7 +235,7 @@ __global__ void k_adj_seed(const double2* x, const double* eps, double2* lam, in
   const double2 v = x[i];
   double2 o = make_double2(0.0, 0.0);
   if (target < 0) {
-    if (eps[i] < 0.0) o = make_double2(-2.0 * v.x, -2.0 * v.y);
+    if (eps[i] >= thr) o = make_double2(2.0 * v.x, 2.0 * v.y);
   } else if (i == target) {
     o = make_double2(2.0 * v.x, 2.0 * v.y);
   }
@@ -424,14 +432,21 @@ int mpc_objective(mpc_ctx* c, const mpc_pulse* p, int K, const double* u, double
     return mpc_fail(MPC_ERR_DEVICE, "kernel status 0x%x during the forward pass", st);
   }
   if (target < 0) {
-    double b = 0.0;
+    double y = 0.0;
     for (int i = 0; i < c->g.ntot; ++i)
-      if (eps[i] < 0.0) b += xN[2 * i] * xN[2 * i] + xN[2 * i + 1] * xN[2 * i + 1];
-    *J = 1.0 - b;
+      if (eps[i] >= c->yield_thr) y += xN[2 * i] * xN[2 * i] + xN[2 * i + 1] * xN[2 * i + 1];
+    *J = y;
   } else {
     *J = xN[2 * target] * xN[2 * target] + xN[2 * target + 1] * xN[2 * target + 1];
   }
   a->have_forward = true;
+  return MPC_OK;
+}
+
+int mpc_objective_threshold(mpc_ctx* c, double thr) {
+  if (!c || !std::isfinite(thr)) return mpc_fail(MPC_ERR_ARG, "bad argument");
+  c->yield_thr = thr;
+  if (c->adj) c->adj->have_forward = false;
   return MPC_OK;
 }
 
@@ -446,7 +461,8 @@ int mpc_objective_backward(mpc_ctx* c, double* grad_u, double* dJdF) {
   const int ntot = c->g.ntot;
   const int nbk = (ntot + 255) / 256;
   int rc;
-  k_adj_seed<<<nbk, 256, 0, c->stream>>>(a->ckpts + n * nseg, c->d_eps, a->lam, a->target, ntot);
+  k_adj_seed<<<nbk, 256, 0, c->stream>>>(a->ckpts + n * nseg, c->d_eps, a->lam, a->target,
+                                    c->yield_thr, ntot);
   CK(cudaGetLastError());
   AdjCombineArgs ac{};
   ac.v = a->v;

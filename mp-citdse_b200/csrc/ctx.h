@@ -70,6 +70,7 @@ struct mpc_ctx {
   struct mpc_resident_state* resident = nullptr;  // resident path (resident.cu)
   struct mpc_batch_res_state* batch_res = nullptr;  // resident batched path (batch_resident.cu)
   int path = 0;  // 0 automatic, 1 streaming, 2 resident (MPC_PATH_*)
+  double yield_thr = 0.0;  // yield objective: 1 - sum over states below this energy
 };
 
 // Launch with programmatic stream serialization (see mpc_tdse.cu).

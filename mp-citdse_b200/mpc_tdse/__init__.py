@@ -93,6 +93,7 @@ def lib():
     L.mpc_profile_enable.argtypes = [C.c_void_p, C.c_int]
     L.mpc_profile_read.argtypes = [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_longlong)]
     L.mpc_batch_rhs.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
+    L.mpc_objective_threshold.argtypes = [C.c_void_p, C.c_double]
     L.mpc_batch_autotune.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]
     L.mpc_batch_propagate.argtypes = [C.c_void_p, C.c_int, C.POINTER(Pulse), _dp, _dp, C.c_double,
                                       C.c_double, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
@@ -311,6 +312,11 @@ class Context:
         return out, {"ground": st[0], "norm": st[1], "yield": st[2], "excited": st[3]}
 
     # -- objective and adjoint gradient -------------------------------------
+    def objective_threshold(self, thr):
+        """Energy below which states count as not ionised in the yield
+        objective (target < 0): J = 1 - sum_{E_i < thr} |c_i|^2 (default 0)."""
+        _check(lib().mpc_objective_threshold(self._h, float(thr)))
+
     def objective(self, pulse, u, T, t0, dt, steps, x0, target=-1, ckpt_every=64):
         """Forward pass; J.  Keeps checkpoints for objective_backward."""
         u = np.ascontiguousarray(u, dtype=np.float64)

@@ -77,6 +77,7 @@ class Oracle:
         L.orc_control_eval.argtypes = [C.c_int, _dp, C.c_double, C.c_double]
         L.orc_tableau.argtypes = [_dp, _dp, _dp, _dp]
         L.orc_use_blas.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_set_yield_threshold.argtypes = [C.c_double]
         L.orc_objective_gradient.argtypes = [C.c_int, _ip, _dp, _dp, C.c_char, C.c_int, _dp,
                                              C.c_int, _dp, C.c_double, C.c_double, C.c_double,
                                              C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]
@@ -160,6 +161,10 @@ class Oracle:
         if rc:
             raise ValueError(f"orc_objective_gradient rc={rc}")
         return J.value, g, fb, xN.view(np.complex128)
+
+    def yield_threshold(self, thr):
+        """Energy below which states count as bound in the yield objective."""
+        self.lib.orc_set_yield_threshold(float(thr))
 
     def objective(self, n, eig, dip, gauge, field_kind, pars, u, T, t0, dt, steps, x0, target=-1):
         n, eig, dip = self._sys(n, eig, dip)

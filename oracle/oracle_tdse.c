@@ -530,8 +530,10 @@ int orc_propagate_adaptive(int L_max, const int *n, const double *eig,
 /*                                                                           */
 /* Forward per step n: F_n = base(t_n+dt) + dE(t_n+dt); y_s, k_s = M(F_n) y_s */
 /* (M = -i(H0 + F S) length, -i H0 + F K velocity); z_n = x_n + h sum b_j k_j;*/
-/* x_{n+1} = z_n / ||z_n||.  Objective J(x_N): target < 0 -> ionisation      */
-/* yield 1 - sum_{eig<0} |x_i|^2; else |x_target|^2.                         */
+/* x_{n+1} = z_n / ||z_n||.  Objective J(x_N): target < 0 -> the yield       */
+/* above the threshold, 1 - sum_{eig<thr} |x_i|^2 (thr = 0 unless            */
+/* orc_set_yield_threshold changed it), evaluated as sum_{eig>=thr} |x_i|^2  */
+/* (||x_N|| = 1) with the seed 2 x on those states; else |x_target|^2.       */
 /* Reverse (real inner product Re<u,v>, M^T = M^dagger = -M):               */
 /*   zbar = (lam - x_{n+1} Re<x_{n+1},lam>) / ||z_n||                        */
 /*   kbar_s = h b_s zbar + sum_{s'>s} h a_{s's} ybar_{s'}  (s = 12..0)       */
@@ -539,6 +541,9 @@ int orc_propagate_adaptive(int L_max, const int *n, const double *eig,
 /*   lam_n = zbar + sum_s ybar_s                                             */
 /* dJ/du_k = sum_n dJ/dF_n * phi((t_n + dt)/g - k).                          */
 /* ------------------------------------------------------------------------ */
+
+static double g_yield_thr = 0.0;
+void orc_set_yield_threshold(double thr) { g_yield_thr = thr; }
 
 /* M1 v (coupling at unit field), with a zero diagonal. */
 static void coupling(const sys_t *s, const double *v, double *out, double *zero_eig) {
@@ -599,12 +604,12 @@ int orc_objective_gradient(int L_max, const int *n, const double *eig, const dou
   if (target < 0) {
     double b = 0.0;
     for (int i = 0; i < s.ntot; ++i)
-      if (eig[i] < 0.0) {
+      if (eig[i] >= g_yield_thr) {
         b += xf[2 * i] * xf[2 * i] + xf[2 * i + 1] * xf[2 * i + 1];
-        lam[2 * i] = -2.0 * xf[2 * i];
-        lam[2 * i + 1] = -2.0 * xf[2 * i + 1];
+        lam[2 * i] = 2.0 * xf[2 * i];
+        lam[2 * i + 1] = 2.0 * xf[2 * i + 1];
       }
-    Jv = 1.0 - b;
+    Jv = b;
   } else {
     Jv = xf[2 * target] * xf[2 * target] + xf[2 * target + 1] * xf[2 * target + 1];
     lam[2 * target] = 2.0 * xf[2 * target];
@@ -673,8 +678,8 @@ int orc_objective(int L_max, const int *n, const double *eig, const double *dip,
   if (target < 0) {
     double b = 0.0;
     for (int i = 0; i < s.ntot; ++i)
-      if (eig[i] < 0.0) b += x[2 * i] * x[2 * i] + x[2 * i + 1] * x[2 * i + 1];
-    Jv = 1.0 - b;
+      if (eig[i] >= g_yield_thr) b += x[2 * i] * x[2 * i] + x[2 * i + 1] * x[2 * i + 1];
+    Jv = b;
   } else {
     Jv = x[2 * target] * x[2 * target] + x[2 * target + 1] * x[2 * target + 1];
   }

@@ -89,3 +89,42 @@ def test_torch_autograd_function():
         J2, g2, _ = ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0)
     assert abs(float(J.detach()) - J2) == 0.0
     assert np.allclose(ut.grad.numpy(), 2.0 * g2, rtol=0, atol=1e-15 * np.max(np.abs(g2)) + 1e-300)
+
+
+@pytest.mark.parametrize("thr", [0.0, -2.0])
+def test_2e_ionisation_yields_match_oracle_and_differences(oracle, thr):
+    """2e He-CI-like system, velocity gauge: the double-ionisation yield
+    (states above the He2+ threshold, thr = 0) and the single-ionisation
+    yield (above He+(1s), thr = -2) and their gradients against the oracle's
+    adjoint, plus one central difference."""
+    from mpc_tdse.systems import helium_like_2e
+
+    s = helium_like_2e((60, 70, 64, 50), gauge="v", seed=3, e_max=8.0)
+    Io, w = mpc_tdse.to_au(8e14, 6.2)
+    tau = mpc_tdse.period(w, 2)
+    p = mpc_tdse.pulse_setup("sine", "v", Io, w, 0.0, 2, tau)
+    rng = np.random.default_rng(11)
+    K = 64
+    u = rng.standard_normal(K) * 0.01 * p.Eo
+    x0 = np.zeros(s.ntot, complex)
+    x0[0] = 1.0
+    steps = int(tau / 0.05)
+    oracle.yield_threshold(thr)
+    try:
+        Jo, go, _, _ = oracle.objective_gradient(s.n, s.eig, s.dip, "v", "sineAA", p.as_array(),
+                                                 u, tau, 0.0, 0.05, steps, x0, -1)
+    finally:
+        oracle.yield_threshold(0.0)
+    with mpc_tdse.Context.from_system(s) as ctx:
+        ctx.objective_threshold(thr)
+        J, gr, _ = ctx.objective_gradient(p, u, tau, 0.0, 0.05, steps, x0, -1)
+        h, k = 1e-6, int(np.argmax(np.abs(go)))   # the largest component: FD error ~3e-7
+        up, um = u.copy(), u.copy()
+        up[k] += h
+        um[k] -= h
+        fd = (ctx.objective(p, up, tau, 0.0, 0.05, steps, x0) -
+              ctx.objective(p, um, tau, 0.0, 0.05, steps, x0)) / (2 * h)
+    assert 0.0 < J < 1.0
+    assert abs(J - Jo) < 1e-12
+    assert np.max(np.abs(gr - go)) <= 1e-9 * np.max(np.abs(go))
+    assert abs(fd - gr[k]) <= 1e-6 * max(abs(fd), 1e-8 * np.max(np.abs(gr)))
