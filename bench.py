@@ -234,6 +234,31 @@ def measure_batched(local, stream_cls, rank=0, world=1, dist=None):
     }
 
 
+def batched_kernel_case(local):
+    """A short batched run for profilers (no autotuning launches, so the
+    launch list is the propagation alone): 256 pulses of the batched workload
+    over t in [0, 1] a.u. (stage GEMM at full width, 64-column tiles), then 4
+    of them over [0, 2] a.u. (the persistent resident kernel)."""
+    import numpy as np
+
+    os.environ["MPC_NO_AUTOTUNE"] = "1"
+    import mpc_tdse
+    from mpc_tdse.structure1e import hydrogen
+
+    s = hydrogen(n=300, k=9, R=200.0, l_max=5, gauge="l", states=[292] * 6)
+    ctx = mpc_tdse.Context.from_system(s, device=local)
+    pulses, _ = batched_pulses(mpc_tdse)
+    X0 = np.zeros((len(pulses), s.ntot), complex)
+    X0[:, 0] = 1.0
+    _, acc, rej, _ = ctx.batch_propagate(pulses, 0.0, [1.0] * len(pulses), X0, h0=0.05,
+                                         dt_max=0.15, rtol=1e-10, atol=1e-10)
+    _, acc4, rej4, _ = ctx.batch_propagate(pulses[:4], 0.0, [2.0] * 4, X0[:4], h0=0.05,
+                                           dt_max=0.15, rtol=1e-10, atol=1e-10)
+    ctx.close()
+    print(f"batched 256 pulses: {int(acc.sum() + rej.sum())} pulse-attempts; "
+          f"resident 4 pulses: {int(acc4.sum() + rej4.sum())} pulse-attempts")
+
+
 def measure_adjoint(local, stream_cls, n_fd=2):
     """Adjoint gradient of the ionisation yield w.r.t. 4096 E(t) control
     samples: 1e H-like, 398 states/l, l = 0..8 (3582 states), length gauge,
@@ -460,9 +485,11 @@ def main():
                     help="skip the adjoint-gradient measurement")
     ap.add_argument("--no-he2e-batched", action="store_true",
                     help="skip the batched + adjoint 2e measurement (30k states, 64 pulses)")
-    ap.add_argument("--mode", default="full", choices=["full", "kernel"],
+    ap.add_argument("--mode", default="full", choices=["full", "kernel", "batched-kernel"],
                     help="kernel: only warm-up + timed steps of the workload (a small case for "
-                         "profilers); no JSON line")
+                         "profilers); batched-kernel: a short batched run (256 pulses at full "
+                         "width, then 4 pulses in the resident kernel) for profilers; no JSON "
+                         "line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -471,6 +498,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.mode == "batched-kernel":
+        batched_kernel_case(local)
         return
 
     import numpy as np
