@@ -203,6 +203,29 @@ int mpc_objective_gradient(mpc_ctx *ctx, const mpc_pulse *pulse, int K, const do
                            double T, double t0, double dt, int steps, int target, int ckpt_every,
                            const double *ct0, double *J, double *grad_u, double *dJdF);
 
+/* Batched objective and gradient (new).  B pulses at once with the semantics
+ * of mpc_objective / mpc_objective_backward per pulse: pulse b has its own
+ * field pulses[b], K controls u[b*K .. b*K+K) on its own window [0, T[b]]
+ * (u and T may be NULL when K == 0), and all share t0, dt, steps, target,
+ * the yield threshold and ckpt_every.  ct0: host [B][2*size]; J: host [B].
+ * The forward and the adjoint stages run as FP64 tensor-core GEMMs over all
+ * pulses (the couplings are read once per stage for the whole batch).
+ * mpc_batch_objective_backward returns grad_u [B][K] and dJdF [B][steps]
+ * (either may be NULL) for the last mpc_batch_objective call.  Device memory:
+ * about (steps/ckpt_every + 13*ckpt_every + 20) x size x 16 x ceil32(B) bytes;
+ * ckpt_every <= 0 picks the longest interval that fits in 85 % of the free
+ * device memory (every step kept, no recomputation, when that fits).  The
+ * forward keeps its last segment, which the backward pass then does not
+ * recompute. */
+int mpc_batch_objective(mpc_ctx *ctx, int B, const mpc_pulse *pulses, int K, const double *u,
+                        const double *T, double t0, double dt, int steps, int target,
+                        int ckpt_every, const double *ct0, double *J);
+int mpc_batch_objective_backward(mpc_ctx *ctx, double *grad_u, double *dJdF);
+int mpc_batch_objective_gradient(mpc_ctx *ctx, int B, const mpc_pulse *pulses, int K,
+                                 const double *u, const double *T, double t0, double dt,
+                                 int steps, int target, int ckpt_every, const double *ct0,
+                                 double *J, double *grad_u, double *dJdF);
+
 /* Photoelectron spectrum and populations of the context's current state
  * (after mpc_propagate / mpc_advance), or of ct (host, 2*size doubles) when
  * non-NULL: pes::genPES1e / genPES2e (src/pes/pes.cpp:48-262) without their

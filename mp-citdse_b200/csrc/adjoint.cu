@@ -242,7 +242,9 @@ __global__ void k_adj_seed(const double2* x, const double* eps, double2* lam, in
   lam[i] = o;
 }
 
-double keys_phi(double s) {
+}  // namespace
+
+static double keys_phi(double s) {
   const double x = std::fabs(s);
   if (x < 1.0) return (1.5 * x - 2.5) * x * x + 1.0;
   if (x < 2.0) return ((-0.5 * x + 2.5) * x - 4.0) * x + 2.0;
@@ -250,7 +252,7 @@ double keys_phi(double s) {
 }
 
 // dE(t) and the 4 weights it takes from the samples (first index in *k0)
-double control_at(int K, const double* u, double T, double t, int* k0, double* w) {
+double mpc_control_at(int K, const double* u, double T, double t, int* k0, double* w) {
   for (int j = 0; j < 4; ++j) w[j] = 0.0;
   *k0 = 0;
   if (K < 2 || t < 0.0 || t > T) return 0.0;
@@ -267,8 +269,6 @@ double control_at(int K, const double* u, double T, double t, int* k0, double* w
   }
   return acc;
 }
-
-}  // namespace
 
 struct mpc_adjoint_state {
   int steps = 0, ckpt = 0, nseg = 0, target = -1, K = 0;
@@ -333,10 +333,10 @@ int ensure_adjoint(mpc_ctx* c, int steps, int ckpt) {
       (rc = aalloc(a, &a->fbar, steps)))
     return rc;
   // zero the padded tails the streaming kernel may read
-  CK(cudaMemset(a->ckpts, 0, sizeof(double2) * n * (nseg + 1)));
-  CK(cudaMemset(a->segX, 0, sizeof(double2) * n * (ckpt + 1)));
-  CK(cudaMemset(a->segY, 0, sizeof(double2) * n * (size_t)ckpt * kNumStages));
-  CK(cudaMemset(a->v, 0, sizeof(double2) * n));
+  CK(cudaMemsetAsync(a->ckpts, 0, sizeof(double2) * n * (nseg + 1), c->stream));
+  CK(cudaMemsetAsync(a->segX, 0, sizeof(double2) * n * (ckpt + 1), c->stream));
+  CK(cudaMemsetAsync(a->segY, 0, sizeof(double2) * n * (size_t)ckpt * kNumStages, c->stream));
+  CK(cudaMemsetAsync(a->v, 0, sizeof(double2) * n, c->stream));
   a->cap_ckpt = nseg + 1;
   a->cap_seg = ckpt;
   a->cap_steps = steps;
@@ -400,7 +400,7 @@ int mpc_objective(mpc_ctx* c, const mpc_pulse* p, int K, const double* u, double
   double w[4];
   for (int st = 0; st < steps; ++st) {
     a->tn[st] = t + dt;
-    a->F[st] = mpc_field(p, t + dt) + (K > 0 ? control_at(K, u, T, t + dt, &k0, w) : 0.0);
+    a->F[st] = mpc_field(p, t + dt) + (K > 0 ? mpc_control_at(K, u, T, t + dt, &k0, w) : 0.0);
     t += dt;
   }
   if ((rc = mpc_fill_field_table(c, a->F.data(), steps))) return rc;
@@ -428,7 +428,7 @@ int mpc_objective(mpc_ctx* c, const mpc_pulse* p, int K, const double* u, double
   unsigned st = 0;
   CK(cudaMemcpy(&st, c->d_status, sizeof st, cudaMemcpyDeviceToHost));
   if (st) {
-    cudaMemset(c->d_status, 0, sizeof(unsigned));
+    cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream);
     return mpc_fail(MPC_ERR_DEVICE, "kernel status 0x%x during the forward pass", st);
   }
   if (target < 0) {
@@ -447,6 +447,7 @@ int mpc_objective_threshold(mpc_ctx* c, double thr) {
   if (!c || !std::isfinite(thr)) return mpc_fail(MPC_ERR_ARG, "bad argument");
   c->yield_thr = thr;
   if (c->adj) c->adj->have_forward = false;
+  mpc_badj_invalidate(c);
   return MPC_OK;
 }
 
@@ -523,7 +524,7 @@ int mpc_objective_backward(mpc_ctx* c, double* grad_u, double* dJdF) {
   unsigned st = 0;
   CK(cudaMemcpy(&st, c->d_status, sizeof st, cudaMemcpyDeviceToHost));
   if (st) {
-    cudaMemset(c->d_status, 0, sizeof(unsigned));
+    cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream);
     return mpc_fail(MPC_ERR_DEVICE, "kernel status 0x%x during the adjoint pass", st);
   }
   if (dJdF) std::copy(fb.begin(), fb.end(), dJdF);
@@ -532,7 +533,7 @@ int mpc_objective_backward(mpc_ctx* c, double* grad_u, double* dJdF) {
     for (int stp = steps - 1; stp >= 0; --stp) {
       int k0;
       double w[4];
-      control_at(a->K, a->u.data(), a->T, a->tn[stp], &k0, w);
+      mpc_control_at(a->K, a->u.data(), a->T, a->tn[stp], &k0, w);
       for (int j = 0; j < 4; ++j)
         if (w[j] != 0.0) grad_u[k0 + j] += fb[stp] * w[j];
     }

@@ -616,7 +616,7 @@ int mpc_batch_res_pmax(mpc_ctx* c) {
       cudaMalloc(&r->bar, sizeof(unsigned) * 2) != cudaSuccess ||
       cudaMemcpy(r->part, parts.data(), sizeof(CtaPart) * G, cudaMemcpyHostToDevice) !=
           cudaSuccess ||
-      cudaMemset(r->bar, 0, sizeof(unsigned) * 2) != cudaSuccess) {
+      cudaMemsetAsync(r->bar, 0, sizeof(unsigned) * 2, c->stream) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }

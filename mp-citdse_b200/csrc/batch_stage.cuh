@@ -1,0 +1,564 @@
+// batch_stage.cuh -- the stage GEMM of the batched propagation, shared by the
+// batched adaptive path (batch.cu) and the batched adjoint (batch_adjoint.cu).
+//
+// The state of B pulses is one matrix [n][ldc] (row = basis state, complex
+// column = pulse), so one right-hand side for all pulses is a real GEMM of
+// the block-tridiagonal coupling (the dipole blocks) with the [n x 2B] stage
+// matrix on the FP64 tensor cores (mma.sync m16n8k8 .f64), with an epilogue
+// fused into its store:
+//   MODE 0 (forward): k_s = M(F) y_s, the next stage input (or, after the last
+//     stage, x_new, the embedded error and per-pulse norm partials);
+//   MODE 1 (adjoint): ybar_s = -M(F) kbar_s, the partial of dJ/dF =
+//     -Re<M1 kbar_s, y_s>, and the next adjoint stage input kbar_{s-1} (or,
+//     after stage 0, lambda_n = zbar + sum_s ybar_s).
+// Each translation unit that includes this header owns its own constant
+// tables and kernel instantiations and sets them up with stage_setup().
+#pragma once
+#include <cuda_runtime.h>
+
+#include "ctx.h"
+#include "dev_util.cuh"
+#include "plan.h"
+#include "rkf78.h"
+
+namespace {
+
+using namespace mpc;
+
+constexpr int BM = 64, BK = 32, BTHREADS = 256;
+constexpr int LDA_P = BM + 4;   // A stored [k][m] (transposed block), pitch in doubles
+constexpr int LDA_Q = BK + 4;   // A stored [m][k]
+constexpr int A_STAGE = (BK * LDA_P > BM * LDA_Q) ? BK * LDA_P : BM * LDA_Q;
+constexpr int kColAlign = 32;   // pulse columns are allocated in multiples of this
+
+// Column-tile shapes (real columns = 2 x pulses).  8 warps in a WGM x WGN
+// grid, each owning WMT x WNT tiles of m16n8; BM = WGM*WMT*16 = 64 rows.
+// The narrowest tile covering the active pulses is used, so that a batch
+// whose pulses have mostly retired does not pay for empty columns.
+template <int BN_> struct Tile;
+// KS: independent accumulator sets rotated by k-step.  Every variant keeps
+// KS = 1 so that all tile shapes sum the coupling in the same order and give
+// bit-identical results: the autotuner's choice never changes the numbers.
+template <> struct Tile<64> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 2, KS = 1; };
+template <> struct Tile<32> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 1, KS = 1; };
+template <> struct Tile<16> { static constexpr int WGM = 4, WGN = 2, WMT = 1, WNT = 1, KS = 1; };
+template <int BN_> constexpr int b_stage() { return BK * (BN_ + 4); }
+// NST_ cp.async stages: 3 for the wide tile (two CTAs per SM), 6 for the
+// narrow ones (small grids: more loads in flight per CTA instead)
+template <int BN_, int NST_> constexpr int batch_smem() {
+  return NST_ * (A_STAGE + b_stage<BN_>()) * 8;
+}
+
+__constant__ double c_A[13][13];
+__constant__ double c_B8[13];
+__constant__ double c_E[13];   // b8 - b7
+__constant__ double c_C[13];
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = smem_u32(smem);
+  const int sz = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(sz)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// D (16x8, f64) += A (16x8) * B (8x8); fragments as in the PTX ISA for
+// m16n8k8 .f64: a = {A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]},
+// b = {B[t][g], B[t+4][g]}, c = {C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]}
+// with g = lane / 4, t = lane % 4.
+__device__ __forceinline__ void dmma16x8x8(double* c, const double* a, const double* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+struct StageArgs {
+  const double* D;
+  const double* eps;
+  const double2* X;      // x, [n][ldc]
+  const double2* Yin;    // y_s (X for s = 0)
+  double2* K;            // k[13][n][ldc]
+  double2* Yout;         // y_{s+1}, or x_new for s = 12
+  const double* Fs;      // stage fields: Fs[s * fs_stride + q]
+  const double* h;       // [ldc] attempt step
+  unsigned long long* err;  // [ldc] bits of the max error ratio
+  double* normpart;      // [nrowtiles][ldc]
+  double rtol, atol;
+  int stage;
+  int gauge;             // 0 length, 1 velocity
+  int ncol;              // active pulse columns
+  int ldc;               // allocated pulse columns (row pitch of X, Y, K in complex)
+  int nrowtiles;
+  int want_k_only;       // 1: stop after storing k_s (single RHS evaluations)
+  int fs_stride;         // ldc (a field per stage) or 0 (one field per step)
+  // adjoint stages (MODE 1): Yin = kbar_s, K = ybar slabs, Yout = kbar_{s-1}
+  // (or lambda_n after stage 0)
+  const double2* Ys;     // the forward stage input y_s
+  const double2* Zbar;   // zbar of the step
+  double* fpart;         // [13][nrowtiles][ldc] partials of dJ/dF
+  Geometry g;
+};
+
+template <int BN, int NSTB, int MODE>
+__global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_constant__ StageArgs a) {
+  extern __shared__ __align__(16) double bsm[];
+  constexpr int WGM = Tile<BN>::WGM, WMT = Tile<BN>::WMT, WNT = Tile<BN>::WNT;
+  constexpr int LDB = BN + 4;
+  constexpr int B_STAGE = b_stage<BN>();
+  constexpr int WM_TILES = WMT, WN_TILES = WNT;
+  static_assert(Tile<BN>::WGM * Tile<BN>::WGN * 32 == BTHREADS, "8 warps");
+  static_assert(WGM * WMT * 16 == BM && Tile<BN>::WGN * WNT * 8 == BN, "tile shape");
+  pdl_trigger();
+  const Geometry& g = a.g;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int wm = warp % WGM, wn = warp / WGM;
+
+  // row tile -> state block L and first local row r0
+  int L = 0, rt = blockIdx.x;
+  while (true) {
+    const int nt = (g.state_off[L + 1] - g.state_off[L] + BM - 1) / BM;
+    if (rt < nt || L + 1 >= g.nstate_blk) break;
+    rt -= nt;
+    ++L;
+  }
+  const int nL = g.state_off[L + 1] - g.state_off[L];
+  const int r0 = rt * BM;
+  const int c0 = blockIdx.y * BN;           // first real column
+  const int ncr = 2 * a.ncol;               // real columns in use
+  const int ldr = 2 * a.ldc;                // real row pitch of X / Y
+  const bool hasP = L > 0, hasQ = L < g.nblk;
+  const int KP = hasP ? g.state_off[L] - g.state_off[L - 1] : 0;
+  const int KQ = hasQ ? g.state_off[L + 2] - g.state_off[L + 1] : 0;
+  const int nchP = (KP + BK - 1) / BK, nchQ = (KQ + BK - 1) / BK;
+  const int nch = nchP + nchQ;
+  const double qsign = (a.gauge == 1) ? -1.0 : 1.0;
+
+  pdl_wait();
+  const double* Yin = reinterpret_cast<const double*>(a.Yin);
+
+  // Each thread's cp.async assignments are fixed for the whole K loop, so
+  // their source pointers and bounds are set up once; a chunk only adds its
+  // k offset.
+  constexpr int A_PER = BK * (BM / 2) / BTHREADS;       // 16-B copies of A per thread
+  constexpr int BPR = BN / 2;                            // 16-B copies per B row
+  constexpr int B_ROWS = BTHREADS / BPR;                 // B rows per pass
+  constexpr int B_PER = (BK + B_ROWS - 1) / B_ROWS;
+  const int tid = threadIdx.x;
+  const int p_mm = 2 * (tid % (BM / 2)), p_kk0 = tid / (BM / 2);   // P: kk = p_kk0 + 8 i
+  const int q_kk = 2 * (tid % (BK / 2)), q_mm0 = tid / (BK / 2);   // Q: mm = q_mm0 + 16 i
+  const int b_nn = 2 * (tid % BPR), b_kk0 = tid / BPR;
+  const bool p_mv = r0 + p_mm < nL;
+  const bool b_nv = c0 + b_nn < ncr;
+  const long long pitchP = hasP ? g.blk[L - 1].pitch : 0;
+  const long long pitchQ = hasQ ? g.blk[L].pitch : 0;
+  const double* p_base = hasP ? a.D + g.blk[L - 1].d_off + r0 + p_mm : a.D;
+  const double* q_base = hasQ ? a.D + g.blk[L].d_off + (long long)(r0 + q_mm0) * pitchQ + q_kk : a.D;
+  const int yrowP = hasP ? g.state_off[L - 1] : 0, yrowQ = hasQ ? g.state_off[L + 1] : 0;
+
+  auto load_chunk = [&](int ch, int st) {
+    double* As = bsm + st * (A_STAGE + B_STAGE);
+    double* Bs = As + A_STAGE;
+    const bool isP = ch < nchP;
+    const int k0 = (isP ? ch : ch - nchP) * BK;
+    const int nK = isP ? KP : KQ;
+    const int yrow0 = isP ? yrowP : yrowQ;
+    if (isP) {
+      // A = D_{L-1}^T : D_{L-1}[k0+kk][r0+mm] -> As[kk][mm]
+#pragma unroll
+      for (int i = 0; i < A_PER; ++i) {
+        const int kk = p_kk0 + (BTHREADS / (BM / 2)) * i;
+        const bool v = p_mv && (k0 + kk < nK);
+        cp_async16(As + kk * LDA_P + p_mm, v ? p_base + (long long)(k0 + kk) * pitchP : a.D, v);
+      }
+    } else {
+      // A = D_L : D_L[r0+mm][k0+kk] -> As[mm][kk]
+#pragma unroll
+      for (int i = 0; i < A_PER; ++i) {
+        const int mm = q_mm0 + (BTHREADS / (BK / 2)) * i;
+        const bool v = (r0 + mm < nL) && (k0 + q_kk < nK);
+        cp_async16(As + mm * LDA_Q + q_kk,
+                   v ? q_base + (long long)((BTHREADS / (BK / 2)) * i) * pitchQ + k0 : a.D, v);
+      }
+    }
+    // B = Y rows of the coupled block: Bs[kk][nn]
+#pragma unroll
+    for (int i = 0; i < B_PER; ++i) {
+      const int kk = b_kk0 + B_ROWS * i;
+      if (kk < BK) {
+        const bool v = b_nv && (k0 + kk < nK);
+        cp_async16(Bs + kk * LDB + b_nn, v ? Yin + (long long)(yrow0 + k0 + kk) * ldr + c0 + b_nn : Yin, v);
+      }
+    }
+  };
+
+  constexpr int KS = Tile<BN>::KS;
+  double acc_k[KS][WM_TILES][WN_TILES][4];
+#pragma unroll
+  for (int q = 0; q < KS; ++q)
+#pragma unroll
+    for (int i = 0; i < WM_TILES; ++i)
+#pragma unroll
+      for (int j = 0; j < WN_TILES; ++j)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc_k[q][i][j][v] = 0.0;
+
+  for (int p = 0; p < NSTB - 1; ++p) {
+    if (p < nch) load_chunk(p, p);
+    cp_commit();
+  }
+  for (int ch = 0; ch < nch; ++ch) {
+    cp_wait<NSTB - 2>();
+    __syncthreads();
+    {
+      const int nx = ch + NSTB - 1;
+      if (nx < nch) load_chunk(nx, nx % NSTB);
+      cp_commit();
+    }
+    const int st = ch % NSTB;
+    const double* As = bsm + st * (A_STAGE + B_STAGE);
+    const double* Bs = As + A_STAGE;
+    const bool isP = ch < nchP;
+    const double sg = isP ? 1.0 : qsign;
+#pragma unroll
+    for (int ks = 0; ks < BK / 8; ++ks) {
+      double af[WM_TILES][4], bf[WN_TILES][2];
+#pragma unroll
+      for (int mt = 0; mt < WM_TILES; ++mt) {
+        const int m = wm * (WMT * 16) + mt * 16 + gq;
+        const int k = ks * 8 + tq;
+        if (isP) {
+          af[mt][0] = As[k * LDA_P + m];
+          af[mt][1] = As[k * LDA_P + m + 8];
+          af[mt][2] = As[(k + 4) * LDA_P + m];
+          af[mt][3] = As[(k + 4) * LDA_P + m + 8];
+        } else {
+          af[mt][0] = sg * As[m * LDA_Q + k];
+          af[mt][1] = sg * As[(m + 8) * LDA_Q + k];
+          af[mt][2] = sg * As[m * LDA_Q + k + 4];
+          af[mt][3] = sg * As[(m + 8) * LDA_Q + k + 4];
+        }
+      }
+#pragma unroll
+      for (int nt = 0; nt < WN_TILES; ++nt) {
+        const int n = wn * (WNT * 8) + nt * 8 + gq;
+        const int k = ks * 8 + tq;
+        bf[nt][0] = Bs[k * LDB + n];
+        bf[nt][1] = Bs[(k + 4) * LDB + n];
+      }
+#pragma unroll
+      for (int mt = 0; mt < WM_TILES; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < WN_TILES; ++nt) dmma16x8x8(acc_k[ks % KS][mt][nt], af[mt], bf[nt]);
+    }
+  }
+  cp_wait<0>();
+  double acc[WM_TILES][WN_TILES][4];
+#pragma unroll
+  for (int i = 0; i < WM_TILES; ++i)
+#pragma unroll
+    for (int j = 0; j < WN_TILES; ++j)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        double t = acc_k[0][i][j][v];
+#pragma unroll
+        for (int q = 1; q < KS; ++q) t += acc_k[q][i][j][v];
+        acc[i][j][v] = t;
+      }
+
+  if constexpr (MODE == 1) {
+    // ---------------- adjoint epilogue ----------------
+    const int s = a.stage;
+    const long long nld = (long long)g.ntot * a.ldc;
+    __shared__ double red_f[BM / 16][BN / 2];
+#pragma unroll
+    for (int nt = 0; nt < WN_TILES; ++nt) {
+      const int q = (c0 + wn * (WNT * 8) + nt * 8) / 2 + tq;  // pulse column
+      const bool qv = q < a.ncol;
+      double fsum[WM_TILES];
+#pragma unroll
+      for (int mt = 0; mt < WM_TILES; ++mt) fsum[mt] = 0.0;
+      const double F = qv ? a.Fs[s * a.fs_stride + q] : 0.0;
+      const double hq = qv ? a.h[q] : 0.0;
+#pragma unroll
+      for (int mt = 0; mt < WM_TILES; ++mt)
+#pragma unroll
+        for (int hr = 0; hr < 2; ++hr) {
+          const int r = r0 + wm * (WMT * 16) + mt * 16 + gq + 8 * hr;
+          if (!qv || r >= nL) continue;
+          const long long i = g.state_off[L] + r;
+          const long long idx = i * a.ldc + q;
+          const double wre = acc[mt][nt][2 * hr], wim = acc[mt][nt][2 * hr + 1];
+          const double2 kb = a.Yin[idx];
+          const double e = a.eps[i];
+          // M(F) kbar (formed as the forward forms k) and M1 kbar = dM/dF kbar
+          double gre, gim, mre, mim;
+          if (a.gauge == 0) {
+            gre = fma(F, wim, e * kb.y);
+            gim = -fma(F, wre, e * kb.x);
+            mre = wim;
+            mim = -wre;
+          } else {
+            gre = fma(F, wre, e * kb.y);
+            gim = fma(F, wim, -e * kb.x);
+            mre = wre;
+            mim = wim;
+          }
+          const double2 yb = make_double2(-gre, -gim);  // ybar_s = -M kbar_s
+          a.K[s * nld + idx] = yb;
+          const double2 y = a.Ys[idx];
+          fsum[mt] -= fma(mre, y.x, mim * y.y);         // -Re<M1 kbar_s, y_s>
+          const double2 zb = a.Zbar[idx];
+          double2 o;
+          if (s > 0) {
+            // kbar_{s-1} = h b_{s-1} zbar + sum_{j >= s} h a_{j, s-1} ybar_j
+            const double cb = hq * c_B8[s - 1];
+            o = make_double2(cb * zb.x, cb * zb.y);
+#pragma unroll
+            for (int j = 1; j < kNumStages; ++j) {
+              const double cj = c_A[j][s - 1];
+              if (j < s || cj == 0.0) continue;
+              const double2 ybj = (j == s) ? yb : a.K[j * nld + idx];
+              const double cf = hq * cj;
+              o.x = fma(cf, ybj.x, o.x);
+              o.y = fma(cf, ybj.y, o.y);
+            }
+          } else {
+            // lambda_n = zbar + sum_j ybar_j
+            o = zb;
+#pragma unroll
+            for (int j = 0; j < kNumStages; ++j) {
+              const double2 ybj = (j == 0) ? yb : a.K[j * nld + idx];
+              o.x += ybj.x;
+              o.y += ybj.y;
+            }
+          }
+          a.Yout[idx] = o;
+        }
+#pragma unroll
+      for (int o = 4; o < 32; o <<= 1)
+#pragma unroll
+        for (int mt = 0; mt < WM_TILES; ++mt)
+          fsum[mt] += __shfl_xor_sync(0xffffffffu, fsum[mt], o);
+      const int col = wn * (WNT * 4) + nt * 4 + tq;
+      if (gq == 0) {
+#pragma unroll
+        for (int mt = 0; mt < WM_TILES; ++mt) red_f[wm * WMT + mt][col] = fsum[mt];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < BN / 2) {
+      const int q = c0 / 2 + threadIdx.x;
+      if (q < a.ncol) {
+        double fs = red_f[0][threadIdx.x];
+#pragma unroll
+        for (int m = 1; m < BM / 16; ++m) fs += red_f[m][threadIdx.x];
+        a.fpart[((long long)s * a.nrowtiles + blockIdx.x) * a.ldc + q] = fs;
+      }
+    }
+    return;
+  }
+
+  // ---------------- fused RK epilogue ----------------
+  const int s = a.stage;
+  const long long nld = (long long)g.ntot * a.ldc;  // complex elements per k slab
+  const bool last = (s == kNumStages - 1);
+  // norm partials per 16-row m-tile, summed over the tile's rows by a fixed
+  // tree and over the row tile's four m-tiles in order: the same association
+  // for every tile shape
+  __shared__ double red_n[BM / 16][BN / 2];
+  __shared__ double red_e[WGM][BN / 2];
+#pragma unroll
+  for (int nt = 0; nt < WN_TILES; ++nt) {
+    const int q = (c0 + wn * (WNT * 8) + nt * 8) / 2 + tq;  // pulse column
+    const bool qv = q < a.ncol;
+    double nsum[WM_TILES], emax = 0.0;
+#pragma unroll
+    for (int mt = 0; mt < WM_TILES; ++mt) nsum[mt] = 0.0;
+    const double F = qv ? a.Fs[s * a.fs_stride + q] : 0.0;
+    const double hq = qv ? a.h[q] : 0.0;
+#pragma unroll
+    for (int mt = 0; mt < WM_TILES; ++mt)
+#pragma unroll
+      for (int hr = 0; hr < 2; ++hr) {
+        const int r = r0 + wm * (WMT * 16) + mt * 16 + gq + 8 * hr;
+        if (!qv || r >= nL) continue;
+        const long long i = g.state_off[L] + r;
+        const long long idx = i * a.ldc + q;
+        const double wre = acc[mt][nt][2 * hr], wim = acc[mt][nt][2 * hr + 1];
+        const double2 y = a.Yin[idx];
+        const double e = a.eps[i];
+        double kre, kim;
+        if (a.gauge == 0) {
+          kre = fma(F, wim, e * y.y);
+          kim = -fma(F, wre, e * y.x);
+        } else {
+          kre = fma(F, wre, e * y.y);
+          kim = fma(F, wim, -e * y.x);
+        }
+        a.K[s * nld + idx] = make_double2(kre, kim);
+        if (a.want_k_only) continue;
+        const double2 x = a.X[idx];
+        double2 o = x;
+        if (!last) {
+#pragma unroll
+          for (int j = 0; j < kNumStages; ++j) {
+            const double cj = c_A[s + 1][j];
+            if (j > s || cj == 0.0) continue;
+            const double2 kj = (j == s) ? make_double2(kre, kim) : a.K[j * nld + idx];
+            const double cf = hq * cj;
+            o.x = fma(cf, kj.x, o.x);
+            o.y = fma(cf, kj.y, o.y);
+          }
+        } else {
+          double2 er = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int j = 0; j < kNumStages; ++j) {
+            const double bj = c_B8[j], ej = c_E[j];
+            if (bj == 0.0 && ej == 0.0) continue;
+            const double2 kj = (j == s) ? make_double2(kre, kim) : a.K[j * nld + idx];
+            if (bj != 0.0) {
+              o.x = fma(hq * bj, kj.x, o.x);
+              o.y = fma(hq * bj, kj.y, o.y);
+            }
+            if (ej != 0.0) {
+              er.x = fma(hq * ej, kj.x, er.x);
+              er.y = fma(hq * ej, kj.y, er.y);
+            }
+          }
+          const double ax = sqrt(x.x * x.x + x.y * x.y), an = sqrt(o.x * o.x + o.y * o.y);
+          const double ae = sqrt(er.x * er.x + er.y * er.y);
+          const double ratio = ae / (a.atol + a.rtol * fmax(ax, an));
+          emax = fmax(emax, ratio);
+          if (!(ratio == ratio)) emax = ratio;  // keep a NaN
+          nsum[mt] += o.x * o.x + o.y * o.y;
+        }
+        a.Yout[idx] = o;
+      }
+    if (last && !a.want_k_only) {
+      // per pulse and m-tile: this thread's two rows, then the 8 lanes
+      // sharing tq (fixed xor tree)
+#pragma unroll
+      for (int o = 4; o < 32; o <<= 1) {
+#pragma unroll
+        for (int mt = 0; mt < WM_TILES; ++mt)
+          nsum[mt] += __shfl_xor_sync(0xffffffffu, nsum[mt], o);
+        const double oe = __shfl_xor_sync(0xffffffffu, emax, o);
+        emax = (oe != oe) ? oe : fmax(emax, oe);
+      }
+      const int col = wn * (WNT * 4) + nt * 4 + tq;  // pulse slot within the CTA
+      if (gq == 0) {
+#pragma unroll
+        for (int mt = 0; mt < WM_TILES; ++mt) red_n[wm * WMT + mt][col] = nsum[mt];
+        red_e[wm][col] = emax;
+      }
+    }
+  }
+  if (last && !a.want_k_only) {
+    __syncthreads();
+    if (threadIdx.x < BN / 2) {
+      const int q = c0 / 2 + threadIdx.x;
+      if (q < a.ncol) {
+        double ns = red_n[0][threadIdx.x], em = red_e[0][threadIdx.x];
+#pragma unroll
+        for (int m = 1; m < BM / 16; ++m) ns += red_n[m][threadIdx.x];
+#pragma unroll
+        for (int w = 1; w < WGM; ++w) {
+          const double e = red_e[w][threadIdx.x];
+          em = (em != em) ? em : ((e != e) ? e : fmax(em, e));
+        }
+        a.normpart[(long long)blockIdx.x * a.ldc + q] = ns;
+        atomicMax(&a.err[q], (unsigned long long)__double_as_longlong(em));
+      }
+    }
+  }
+}
+
+
+// Stage-GEMM variants: pulse-column tile width (real columns) and cp.async
+// pipeline depth.  Three-stage variants fit two CTAs per SM.
+struct TileVariant {
+  int bn, nst;
+};
+constexpr TileVariant kVariants[] = {{16, 3}, {16, 6}, {32, 3}, {32, 6}, {64, 3}};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+inline int width_bucket(int ncol) {
+  int j = 0;
+  while ((1 << j) < ncol) ++j;
+  return j;
+}
+
+// Before tuning: the narrowest tile that covers the pulses.
+inline int default_variant(int ncol) {
+  const int ncr = 2 * ncol;
+  return ncr <= 16 ? 1 : (ncr <= 128 ? 3 : 4);
+}
+
+template <int BN, int NST, int MODE>
+cudaError_t launch_tile(cudaStream_t st, const StageArgs& a) {
+  const int ncr = 2 * a.ncol;
+  return mpc_launch_pdl(k_batch_stage<BN, NST, MODE>, dim3(a.nrowtiles, (ncr + BN - 1) / BN),
+                        dim3(BTHREADS), batch_smem<BN, NST>(), st, a);
+}
+
+template <int MODE>
+cudaError_t launch_variant(cudaStream_t st, int v, const StageArgs& a) {
+  switch (v) {
+    case 0: return launch_tile<16, 3, MODE>(st, a);
+    case 1: return launch_tile<16, 6, MODE>(st, a);
+    case 2: return launch_tile<32, 3, MODE>(st, a);
+    case 3: return launch_tile<32, 6, MODE>(st, a);
+    default: return launch_tile<64, 3, MODE>(st, a);
+  }
+}
+
+template <int MODE>
+cudaError_t set_stage_attrs() {
+  cudaError_t e;
+#define MPC_STAGE_ATTR(BN, NST)                                                          \
+  if ((e = cudaFuncSetAttribute(k_batch_stage<BN, NST, MODE>,                            \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,             \
+                                batch_smem<BN, NST>())) != cudaSuccess)                  \
+    return e;
+  MPC_STAGE_ATTR(16, 3)
+  MPC_STAGE_ATTR(16, 6)
+  MPC_STAGE_ATTR(32, 3)
+  MPC_STAGE_ATTR(32, 6)
+  MPC_STAGE_ATTR(64, 3)
+#undef MPC_STAGE_ATTR
+  return cudaSuccess;
+}
+
+// This translation unit's tableau constants and kernel attributes, once per
+// device.
+inline int stage_setup(int device) {
+  static bool done[64] = {};
+  if (device < 0 || device >= 64) return mpc_fail(MPC_ERR_ARG, "device %d", device);
+  if (done[device]) return MPC_OK;
+  double A[13][13], B8[13], E[13], Cn[13];
+  for (int i = 0; i < 13; ++i) {
+    for (int j = 0; j < 13; ++j) A[i][j] = rkf78::A[i][j];
+    B8[i] = rkf78::B8[i];
+    E[i] = rkf78::B8[i] - rkf78::B7[i];
+    Cn[i] = rkf78::C[i];
+  }
+  CK(cudaMemcpyToSymbol(c_A, A, sizeof A));
+  CK(cudaMemcpyToSymbol(c_B8, B8, sizeof B8));
+  CK(cudaMemcpyToSymbol(c_E, E, sizeof E));
+  CK(cudaMemcpyToSymbol(c_C, Cn, sizeof Cn));
+  CK(set_stage_attrs<0>());
+  CK(set_stage_attrs<1>());
+  done[device] = true;
+  return MPC_OK;
+}
+
+inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace

@@ -69,6 +69,7 @@ struct mpc_ctx {
   struct mpc_adjoint_state* adj = nullptr;  // adjoint work space (adjoint.cu)
   struct mpc_resident_state* resident = nullptr;  // resident path (resident.cu)
   struct mpc_batch_res_state* batch_res = nullptr;  // resident batched path (batch_resident.cu)
+  struct mpc_badj_state* badj = nullptr;  // batched objective / adjoint (batch_adjoint.cu)
   int path = 0;  // 0 automatic, 1 streaming, 2 resident (MPC_PATH_*)
   double yield_thr = 0.0;  // yield objective: 1 - sum over states below this energy
 };
@@ -105,6 +106,11 @@ void mpc_adjoint_free(mpc_ctx* c);
 bool mpc_resident_setup(mpc_ctx* c);
 void mpc_resident_free(mpc_ctx* c);
 void mpc_batch_res_free(mpc_ctx* c);
+void mpc_badj_free(mpc_ctx* c);
+void mpc_badj_invalidate(mpc_ctx* c);  // a setting changed: backward needs a new forward
+// Stage-GEMM variant for ncol active pulses: autotuned if the context's
+// batched path has been tuned, else the default (batch.cu).
+int mpc_batch_variant(mpc_ctx* c, int ncol);
 int mpc_resident_run(mpc_ctx* c, double dt, int steps, int pop_index);
 
 // Launch helpers of the single-pulse path (mpc_tdse.cu), used by adjoint.cu.
@@ -114,3 +120,8 @@ int mpc_launch_combine_x(mpc_ctx* c, const double2* x, int stage, int step, doub
 int mpc_launch_renorm_to(mpc_ctx* c, double2* x_out, const double2* xnew, int step, int pop_index,
                          double* pop_hist, double* norm_hist, int hist_base);
 int mpc_fill_field_table(mpc_ctx* c, const double* F, int steps);
+
+// The control perturbation dE(t) = sum_k u_k phi(t/g - k), g = T/(K-1), phi
+// the Keys (a = -1/2) cubic kernel, zero outside [0, T]; w[0..3] receive the
+// weights of samples k0 .. k0+3 (adjoint.cu).
+double mpc_control_at(int K, const double* u, double T, double t, int* k0, double* w);

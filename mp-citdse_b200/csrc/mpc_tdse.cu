@@ -569,6 +569,7 @@ int mpc_ctx_destroy(mpc_ctx* c) {
   mpc_adjoint_free(c);
   mpc_resident_free(c);
   mpc_batch_res_free(c);
+  mpc_badj_free(c);
   free_all(c);
   for (auto& v : c->ev)
     for (auto& pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }

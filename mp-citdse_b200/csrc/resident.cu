@@ -381,7 +381,7 @@ bool mpc_resident_setup(mpc_ctx* c) {
     cudaGetLastError();
     return false;
   }
-  cudaMemset(r->bar, 0, sizeof(unsigned) * 2);
+  cudaMemsetAsync(r->bar, 0, sizeof(unsigned) * 2, c->stream);
   r->G = G;
   r->smem = smem;
   r->ok = true;

@@ -94,6 +94,10 @@ def lib():
     L.mpc_profile_read.argtypes = [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_longlong)]
     L.mpc_batch_rhs.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
     L.mpc_objective_threshold.argtypes = [C.c_void_p, C.c_double]
+    L.mpc_batch_objective.argtypes = [C.c_void_p, C.c_int, C.POINTER(Pulse), C.c_int, _dp, _dp,
+                                      C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp,
+                                      _dp]
+    L.mpc_batch_objective_backward.argtypes = [C.c_void_p, _dp, _dp]
     L.mpc_batch_autotune.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]
     L.mpc_batch_propagate.argtypes = [C.c_void_p, C.c_int, C.POINTER(Pulse), _dp, _dp, C.c_double,
                                       C.c_double, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
@@ -333,6 +337,38 @@ class Context:
         f = np.zeros(self._adj_steps)
         _check(lib().mpc_objective_backward(self._h, _ptr(g), _ptr(f)))
         return g, f
+
+    def batch_objective(self, pulses, U, T, t0, dt, steps, X0, target=-1, ckpt_every=64):
+        """Objective of B pulses at once (fixed step); U: [B, K] controls,
+        T: [B] control windows; X0: [B, size] start states.  Returns J [B]
+        and keeps checkpoints for batch_objective_backward."""
+        B = len(pulses)
+        arr = (Pulse * B)(*pulses)
+        U = np.ascontiguousarray(np.asarray(U, dtype=np.float64).reshape(B, -1))
+        K = U.shape[1]
+        T = np.ascontiguousarray(np.broadcast_to(np.asarray(T, dtype=np.float64), (B,)))
+        xf = np.ascontiguousarray(X0, dtype=np.complex128).view(np.float64).reshape(B, -1).copy()
+        J = np.zeros(B)
+        _check(lib().mpc_batch_objective(self._h, B, arr, K, _ptr(U) if K else None,
+                                         _ptr(T) if K else None, float(t0), float(dt),
+                                         int(steps), int(target), int(ckpt_every), _ptr(xf),
+                                         _ptr(J)))
+        self._badj = (B, K, int(steps))
+        return J
+
+    def batch_objective_backward(self):
+        """(dJ/du [B, K], dJ/dF_n [B, steps]) of the last batch_objective."""
+        B, K, steps = self._badj
+        G = np.zeros((B, max(K, 1)))
+        Fb = np.zeros((B, steps))
+        _check(lib().mpc_batch_objective_backward(self._h, _ptr(G), _ptr(Fb)))
+        return G[:, :K], Fb
+
+    def batch_objective_gradient(self, pulses, U, T, t0, dt, steps, X0, target=-1,
+                                 ckpt_every=64):
+        J = self.batch_objective(pulses, U, T, t0, dt, steps, X0, target, ckpt_every)
+        G, Fb = self.batch_objective_backward()
+        return J, G, Fb
 
     def objective_gradient(self, pulse, u, T, t0, dt, steps, x0, target=-1, ckpt_every=64):
         J = self.objective(pulse, u, T, t0, dt, steps, x0, target, ckpt_every)
