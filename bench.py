@@ -302,8 +302,29 @@ def measure_adjoint(local, stream_cls, n_fd=2):
              ctx.objective(p, um, tau, 0.0, dt, steps, x0)) / (2 * h)
         fd.append({"k": int(k), "adjoint": float(g[k]), "central_fd": float(d),
                    "rel_err": float(abs(d - g[k]) / max(abs(d), 1e-300))})
+    # batched: 64 seeded control sets on the same pulse over the first 1000
+    # steps (one memory-sized segment), against the single-pulse rate there
+    Bb, win = 64, 1000
+    Ub = rng.standard_normal((Bb, K)) * 0.01 * p.Eo
+    Xb = np.zeros((Bb, s.ntot), complex)
+    Xb[:, 0] = 1.0
+    Tw = np.full(Bb, tau)
+    ctx.batch_autotune(Bb)
+    ctx.batch_objective([p] * Bb, Ub, Tw, 0.0, dt, 4, Xb, -1, 0)   # allocations
+    b0 = time.perf_counter()
+    ctx.batch_objective([p] * Bb, Ub, Tw, 0.0, dt, win, Xb, -1, 0)
+    b1 = time.perf_counter()
+    Gb, _ = ctx.batch_objective_backward()
+    b2 = time.perf_counter()
+    single_win = steps / win / (fwd + bwd)   # single-pulse gradients/s over the same window
+    batched = {"value": Bb / (b2 - b0), "unit": "gradients/s", "pulses": Bb,
+               "window_steps": win, "forward_s": b1 - b0, "gradient_s": b2 - b0,
+               "cost_vs_batched_forward": (b2 - b0) / (b1 - b0),
+               "single_pulse_same_window": single_win,
+               "ratio_vs_single_pulse": Bb / (b2 - b0) / single_win}
     ctx.close()
     return {
+        "batched": batched,
         "workload": "1e hydrogen (400 B-splines, R=200; 388 states/l below 20 a.u., l=0..8: "
                     "3492 states), length gauge, sin^2 800 nm 1e14 W/cm^2 10 cycles, dt=0.05 "
                     "(%d steps, inside the RKF78 stability interval with the field coupling); "
@@ -325,7 +346,8 @@ def measure_he2e_batched(local, stream_cls, window=3.0, adj_T=10.0, K=1024):
     first `window` a.u. against the plain single-pulse path (fixed dt = 0.1);
     then the gradient of the double-ionisation yield (states above the He2+
     threshold) w.r.t. K piecewise-cubic E(t) controls over [0, adj_T] for one
-    pulse, with one central-difference check."""
+    pulse, with one central-difference check, and for all 64 pulses at once
+    (batched adjoint on the stage GEMM)."""
     import time
 
     import numpy as np
@@ -388,9 +410,27 @@ def measure_he2e_batched(local, stream_cls, window=3.0, adj_T=10.0, K=1024):
     um[k] -= h
     fd = (ctx.objective(p, up, adj_T, 0.0, dt, steps, X0[0]) -
           ctx.objective(p, um, adj_T, 0.0, dt, steps, X0[0])) / (2 * h)
+    # batched adjoint: all 64 pulses, each with its own 1024 controls
+    U = np.random.default_rng(4).standard_normal((B, K)) * 0.01 * \
+        np.array([q.Eo for q in pulses])[:, None]
+    Tb = np.full(B, adj_T)
+    ctx.batch_objective(pulses, U, Tb, 0.0, dt, 4, X0, -1, 0)   # allocations
+    b0 = time.perf_counter()
+    Jb = ctx.batch_objective(pulses, U, Tb, 0.0, dt, steps, X0, -1, 0)
+    b1 = time.perf_counter()
+    Gb, _ = ctx.batch_objective_backward()
+    b2 = time.perf_counter()
     ctx.close()
     fwd, grad = t1 - t0, t2 - t0
     return {
+        "batched_adjoint": {"value": B / (b2 - b0), "unit": "gradients/s", "pulses": B,
+                            "controls_per_pulse": K, "steps": steps,
+                            "forward_s": b1 - b0, "gradient_s": b2 - b0,
+                            "cost_vs_batched_forward": (b2 - b0) / (b1 - b0),
+                            "ratio_vs_single_pulse_adjoint": (B / (b2 - b0)) * grad,
+                            "yields": [float(Jb.min()), float(Jb.max())],
+                            "checkpoints": "sized to free device memory (one segment here: "
+                                           "no recomputation)"},
         "workload": "He-CI-like 2e, L=0..4 (30000 states; blocks 5200/5800/6200/6400/6400), "
                     "velocity gauge, energies up to 15 a.u.; 64 pulses (seed 2) I 1e14-1e15 "
                     "W/cm^2, 200-800 nm, sin^2 8 cycles; batched adaptive RKF78 rtol=atol=1e-10 "

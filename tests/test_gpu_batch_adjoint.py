@@ -140,3 +140,23 @@ def test_batch_objective_needs_forward_before_backward():
         with pytest.raises(mpc_tdse.MpcError):
             ctx._badj = (1, 4, 10)
             ctx.batch_objective_backward()
+
+
+def test_batch_torch_autograd_function():
+    import torch
+
+    from mpc_tdse.autograd import BatchControlProblem, batch_control_objective
+
+    s = hydrogen_like_1e(30, 3, gauge="l", seed=8)
+    pulses, U, T = _batch("l", B=4, K=20, seed=2)
+    X0 = np.zeros((4, s.ntot), complex)
+    X0[:, 0] = 1.0
+    w = np.array([1.0, -2.0, 0.5, 3.0])
+    with mpc_tdse.Context.from_system(s) as ctx:
+        prob = BatchControlProblem(ctx, pulses, T, 0.0, 0.1, 150, X0)
+        Ut = torch.tensor(U, dtype=torch.float64, requires_grad=True)
+        J = batch_control_objective(Ut, prob)
+        (torch.from_numpy(w) * J).sum().backward()
+        J2, G2, _ = ctx.batch_objective_gradient(pulses, U, T, 0.0, 0.1, 150, X0)
+    assert np.array_equal(J.detach().numpy(), J2)
+    assert np.array_equal(Ut.grad.numpy(), w[:, None] * G2)
