@@ -10,6 +10,10 @@
 // names, headers, number formats and 10 % checkpoints.  Differences: fewer
 // than 10 steps does not divide by zero (dumps every step); an unknown gauge
 // or missing -e is reported instead of silently doing nothing.
+// Addition: -p also writes every coefficient dump as <pot>_ct_<t>.h5
+// (datasets "ct" [size x 2] and "t" [1], full float64), and -s accepts such a
+// file: a restart from it continues bit for bit, where the 6-digit text dump
+// and the time parsed from its file name lose precision.
 #include <getopt.h>
 #include <unistd.h>
 
@@ -84,6 +88,17 @@ void write_ct(const std::string& prefix, double t, const std::vector<double>& ct
   for (size_t k = 0; k < ct.size(); k += 2) f << k / 2 << "  " << ct[k] << "  " << ct[k + 1] << "\n";
 }
 
+// Full-precision dump: the coefficients and the exact time.
+void write_ct_h5(const std::string& prefix, double t, const std::vector<double>& ct) {
+  const uint64_t n = ct.size() / 2;
+  h5::write(prefix + "_ct_" + std::to_string(t) + ".h5",
+            {{"ct", {n, 2}, ct.data()}, {"t", {1}, &t}});
+}
+
+bool ends_with(const std::string& s, const std::string& suf) {
+  return s.size() >= suf.size() && s.compare(s.size() - suf.size(), suf.size(), suf) == 0;
+}
+
 // tdrd::readInitCt: lines of "index re im", leading blanks and # lines skipped
 void read_init_ct(const std::string& file, int ct_sz, std::vector<double>& ct) {
   std::ifstream fl(file);
@@ -116,8 +131,9 @@ int check(int rc) {
 int run(int argc, char* argv[]) {
   std::string opt_file, out_dir, init_ct = "ground";
   int e_num = 0, pop_n = 0, pop_l = 0;
+  bool h5_dumps = false;
   for (;;) {
-    switch (getopt(argc, argv, "he:f:o:s:n:l:")) {
+    switch (getopt(argc, argv, "he:f:o:s:n:l:p")) {
       case 'h':
         std::cout << "Program for propagating either the 1- or 2-e^- tdse\n"
                   << "-e <1 or 2> the number of electrons in the tdse\n"
@@ -125,7 +141,8 @@ int run(int argc, char* argv[]) {
                   << "-o <path> output directory for the coefficient files\n"
                   << "-s <path> file with the start coefficients\n"
                   << "-n <int> primary quantum number of state to track\n"
-                  << "-l <int> angular quantum number of state to track\n";
+                  << "-l <int> angular quantum number of state to track\n"
+                  << "-p also write full-precision <pot>_ct_<t>.h5 dumps (-s accepts them)\n";
         return -1;
       case 'e':
         e_num = std::stoi(optarg);
@@ -146,6 +163,7 @@ int run(int argc, char* argv[]) {
         --pop_n;
         continue;
       case 'l': pop_l = std::stoi(optarg); continue;
+      case 'p': h5_dumps = true; continue;
     }
     break;
   }
@@ -215,7 +233,16 @@ int run(int argc, char* argv[]) {
   std::vector<double> ct(2 * (size_t)ct_sz, 0.0);
   ct[0] = 1.0;
   double t = 0.0;
-  if (init_ct != "ground") {
+  if (init_ct != "ground" && ends_with(init_ct, ".h5")) {
+    const h5::Dataset c = h5::read(init_ct, "ct");
+    const h5::Dataset tt = h5::read(init_ct, "t");
+    if (c.dims.size() != 2 || c.dims[1] != 2 || c.dims[0] < (uint64_t)ct_sz || tt.data.empty())
+      throw std::runtime_error(init_ct + ": expected ct [>= " + std::to_string(ct_sz) +
+                               " x 2] and t");
+    std::copy(c.data.begin(), c.data.begin() + 2 * (size_t)ct_sz, ct.begin());
+    t = tt.data[0];
+    std::cout << "Start time (a.u.): " << t << "\n";
+  } else if (init_ct != "ground") {
     const std::string fln = fs::path(init_ct).filename();
     const auto t_start = fln.find_first_of("0123456789");
     t = std::stod(fln.substr(t_start));
@@ -238,6 +265,7 @@ int run(int argc, char* argv[]) {
   // output of tdse::propV / propL (src/tdse/tdse.cpp:150-222)
   const int print = steps / 10 > 0 ? steps / 10 : 1;
   write_ct(prefix, t, ct);
+  if (h5_dumps) write_ct_h5(prefix, t, ct);
   std::fstream field_fl(prefix + "_field.dat", std::ios::out);
   field_fl << "#time (a.u.), field (A(t) or E(t)) (a.u.)\n";
   std::fstream f_pop(prefix + "_pop" + std::to_string(pop_n + 1) + std::to_string(pop_l) + ".dat",
@@ -264,10 +292,12 @@ int run(int argc, char* argv[]) {
       std::cout << fld[n - 1] << "\n";
       check(mpc_state_get(ctx, ct.data()));
       write_ct(prefix, t, ct);
+      if (h5_dumps) write_ct_h5(prefix, t, ct);
     }
   }
   check(mpc_state_get(ctx, ct.data()));
   write_ct(prefix, t, ct);
+  if (h5_dumps) write_ct_h5(prefix, t, ct);
   mpc_ctx_destroy(ctx);
   return 0;
 }

@@ -106,3 +106,36 @@ def test_cli_2e_velocity_gauge_matches_reference_files(tmp_path):
 def test_cli_rejects_bad_arguments(tmp_path):
     r = _run(tmp_path, "-e", "3", "-f", "x.yaml", "-o", "out")
     assert r.returncode != 0 and "Invalid number of electrons" in r.stdout
+
+
+def test_cli_full_precision_restart_is_bit_exact(tmp_path):
+    """-p writes <pot>_ct_<t>.h5 next to every text dump; restarting from one
+    (-s file.h5) continues bit for bit: every later dump equals the
+    uninterrupted run's."""
+    s = hydrogen_like_1e(40, 3, gauge="l", seed=5)
+    io.write_inputs(tmp_path, s, "h", electrons=1, pad=4)
+    shutil.copy(os.path.join(GOLDEN, "settings_1e.yaml"), tmp_path / "h.yaml")
+    r = _run(tmp_path, "-e", "1", "-f", "h.yaml", "-o", "out", "-p")
+    assert r.returncode == 0, r.stderr
+    h5s = sorted((f for f in os.listdir(tmp_path / "out") if f.endswith(".h5")),
+                 key=lambda f: float(f.split("_ct_")[1][:-3]))
+    txt = [f for f in os.listdir(tmp_path / "out") if f.endswith(".dat") and "_ct_" in f]
+    assert len(h5s) == len(txt) >= 10
+    # the h5 dump holds the text dump's numbers at full precision
+    _, c_txt = io.read_ct(tmp_path / "out" / h5s[3].replace(".h5", ".dat"))
+    c_h5 = io.h5_read(tmp_path / "out" / h5s[3], "ct")
+    assert c_h5.shape == (s.ntot, 2)
+    assert np.max(np.abs(c_h5[:, 0] + 1j * c_h5[:, 1] - c_txt)) <= 1e-6
+    r2 = _run(tmp_path, "-e", "1", "-f", "h.yaml", "-o", "out2", "-p", "-s", f"out/{h5s[3]}")
+    assert r2.returncode == 0, r2.stderr
+    # the restarted run dumps every tenth of its own (shorter) run: compare the
+    # dumps both runs wrote, the final state among them
+    later = sorted((f for f in os.listdir(tmp_path / "out2") if f.endswith(".h5")),
+                   key=lambda f: float(f.split("_ct_")[1][:-3]))
+    common = [f for f in later if f in h5s]
+    assert h5s[3] in common and later[-1] == h5s[-1] and len(common) >= 2
+    for f in common:
+        a = io.h5_read(tmp_path / "out2" / f, "ct")
+        b = io.h5_read(tmp_path / "out" / f, "ct")
+        assert np.array_equal(a, b), f
+        assert io.h5_read(tmp_path / "out2" / f, "t")[0] == io.h5_read(tmp_path / "out" / f, "t")[0]
