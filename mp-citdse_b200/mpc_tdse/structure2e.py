@@ -185,7 +185,9 @@ class Radial:
             lo = np.einsum("bgm,dgm,gm->bdg", Pbi, Pdi, wlo)    # int over each gap of r^k rho
             hi = np.einsum("bgm,dgm,gm->bdg", Pbi, Pdi, whi)
             cl = np.cumsum(lo, axis=-1)[..., :-1]                # int_0^{r_i}
-            ch = hi.sum(axis=-1, keepdims=True) - np.cumsum(hi, axis=-1)[..., :-1]
+            # int_{r_i}^R summed from R inwards: the r^-(k+1) weight makes the
+            # innermost gaps large, and total - cumsum would cancel them away
+            ch = np.flip(np.cumsum(np.flip(hi, -1), axis=-1), -1)[..., 1:]
             return cl * r ** (-(k + 1.0)) + ch * r ** k
         import torch
 
@@ -194,7 +196,7 @@ class Radial:
         lo = torch.einsum("bgm,dgm,gm->bdg", Pbi_, Pdi_, t(wlo))
         hi = torch.einsum("bgm,dgm,gm->bdg", Pbi_, Pdi_, t(whi))
         cl = torch.cumsum(lo, dim=-1)[..., :-1]
-        ch = hi.sum(dim=-1, keepdim=True) - torch.cumsum(hi, dim=-1)[..., :-1]
+        ch = torch.flip(torch.cumsum(torch.flip(hi, [-1]), dim=-1), [-1])[..., 1:]
         return cl * t(r ** (-(k + 1.0))) + ch * t(r ** k)
 
 

@@ -95,3 +95,16 @@ def test_files_in_reference_layout(tmp_path):
     assert np.array_equal(D, p["D_CI"][0])
     # velocity-gauge CI dipoles couple the ground state to 1P states
     assert np.abs(D[0]).max() > 0.1
+
+
+def test_outer_potential_is_summed_stably():
+    """High box states of high l carry small-r noise that r^-(k+1) amplifies;
+    the outer part of chi must be summed inwards, not as total minus a
+    cumulative sum (which left R^6 of (5f,6f; 100f,100f) at -2e5 and a
+    spurious CI state at -15 a.u.)."""
+    t, Es, Cs = solve_1e(120, 9, 60.0, 2.0, 3, 0.5, glq=15)
+    rad = s2.Radial(t, 9, Cs, 60.0, 100)
+    a = np.array
+    for k in (4, 5, 6):
+        R = s2.slater_block(rad, k, 3, a([5]), 3, a([6]), 3, a([99]), 3, a([99]))[0, 0, 0, 0]
+        assert abs(R) < 1e-2, (k, R)
