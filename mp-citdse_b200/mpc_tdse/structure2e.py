@@ -408,3 +408,45 @@ def write_2e_files(root, pot, parts, gauge):
         write_cfg(os.path.join(dat, f"cfg-{L}.inp"), L, parts["lines"][L])
     for L, D in enumerate(parts["D_CI"]):
         io.h5_write(os.path.join(dat, f"{pot}CI_{L}{L + 1}{gauge}.h5"), {"CI_dip": D})
+
+
+def main(argv=None):
+    """python -m mpc_tdse.structure2e: writes dat/ inputs for `tdse -e 2`
+    (the reference's h1e/w1e/d1e + id2ec/r12/d2e/w2e sequence) and prints the
+    time each stage took."""
+    import argparse
+    import time
+
+    from .structure1e import write_1e_files
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--out", default=".")
+    ap.add_argument("--pot", default="he")
+    ap.add_argument("--n", type=int, default=80, help="B-splines")
+    ap.add_argument("--R", type=float, default=40.0, help="box radius (a.u.)")
+    ap.add_argument("--Z", type=float, default=2.0)
+    ap.add_argument("--lmax", type=int, default=2, help="largest 1e l")
+    ap.add_argument("--Lmax", type=int, default=2, help="largest total L")
+    ap.add_argument("--inner", type=int, default=8, help="inner-electron states per l")
+    ap.add_argument("--outer", type=int, default=60, help="outer-electron states per l")
+    ap.add_argument("--gauge", default="v", choices=["l", "v"])
+    ap.add_argument("--k-max", default="reference")
+    ap.add_argument("--device", default=None, help="torch device, e.g. cuda")
+    a = ap.parse_args(argv)
+    t0 = time.time()
+    write_1e_files(a.out, a.pot, a.n, 9, a.R, a.Z, a.lmax, (a.gauge,))
+    t1 = time.time()
+    _, parts = helium(a.n, 9, a.R, a.Z, a.lmax, a.Lmax, a.inner, a.outer, a.gauge,
+                      a.k_max if a.k_max in ("reference", "complete") else int(a.k_max),
+                      device=a.device)
+    t2 = time.time()
+    write_2e_files(a.out, a.pot, parts, a.gauge)
+    sizes = [len(E) for E in parts["E_CI"]]
+    print(f"configurations per L: {sizes} (total {sum(sizes)})")
+    print(f"ground state energy (a.u.): {parts['E_CI'][0][0]:.8f}")
+    print(f"1e structure {t1 - t0:.2f} s, 2e CI (V12, dipoles, diagonalisation) {t2 - t1:.2f} s"
+          f" on {a.device or 'cpu'}")
+
+
+if __name__ == "__main__":
+    main()
