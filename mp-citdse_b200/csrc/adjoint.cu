@@ -30,7 +30,11 @@
 // Memory: the forward keeps x every `ckpt` steps; the reverse pass re-runs
 // each segment forward from its checkpoint, keeping the segment's states,
 // stage inputs y_s and norms, then walks it backwards.  Cost: one forward,
-// one recomputed forward, one adjoint sweep (about 3 forwards).
+// one recomputed forward, one adjoint sweep (about 3 forwards).  When the
+// couplings fit in shared memory (the resident path) each pass is one
+// persistent launch (resident.cu: the forward with checkpoint / segment
+// outputs, and k_adj_resident for the sweep); otherwise the streamed kernels
+// below run step by step.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -289,6 +293,7 @@ struct mpc_adjoint_state {
   size_t cap_ckpt = 0, cap_seg = 0, cap_steps = 0;
   std::vector<void*> allocs;
   bool have_forward = false;
+  bool resident = false;      // both passes on the shared-memory-resident kernels
 };
 
 namespace {
@@ -412,12 +417,21 @@ int mpc_objective(mpc_ctx* c, const mpc_pulse* p, int K, const double* u, double
   for (int s = 1; s <= 13; ++s) ys[s] = a->segY + n * (s - 1);  // scratch: slots of step 0
   ys[0] = nullptr;
   const double2* x = a->ckpts;
-  for (int st = 0; st < steps; ++st) {
-    double2* xn = ((st + 1) % ckpt_every == 0 || st + 1 == steps)
-                      ? a->ckpts + n * ((st + 1 + ckpt_every - 1) / ckpt_every)
-                      : a->segX + n * ((st & 1) ? 0 : 1);
-    if ((rc = fwd_step(c, st, dt, x, ys, xn, a->segN))) return rc;
-    x = xn;
+  a->resident = mpc_use_resident(c) && mpc_resident_adjoint_ok(c);
+  if (a->resident) {
+    // one persistent launch; it stores the checkpoints as it passes them
+    if ((rc = mpc_resident_forward_ex(c, a->ckpts, a->ckpts + n * a->nseg, c->d_Ftab, dt, steps,
+                                      nullptr, nullptr, nullptr, a->ckpts, ckpt_every,
+                                      (long long)n)))
+      return rc;
+  } else {
+    for (int st = 0; st < steps; ++st) {
+      double2* xn = ((st + 1) % ckpt_every == 0 || st + 1 == steps)
+                        ? a->ckpts + n * ((st + 1 + ckpt_every - 1) / ckpt_every)
+                        : a->segX + n * ((st & 1) ? 0 : 1);
+      if ((rc = fwd_step(c, st, dt, x, ys, xn, a->segN))) return rc;
+      x = xn;
+    }
   }
   // objective on the host from x_N
   std::vector<double> xN(2 * c->g.ntot), eps(c->g.ntot);
@@ -482,6 +496,16 @@ int mpc_objective_backward(mpc_ctx* c, double* grad_u, double* dJdF) {
   for (int seg = nseg - 1; seg >= 0; --seg) {
     const int n0 = seg * ckpt;
     const int len = std::min(ckpt, steps - n0);
+    if (a->resident) {
+      // recompute the segment (states, stage inputs, norms), then its sweep
+      if ((rc = mpc_resident_forward_ex(c, a->ckpts + n * seg, a->segX + n * len,
+                                        c->d_Ftab + n0, dt, len, a->segX, a->segY, a->segN,
+                                        nullptr, 0, (long long)n)) ||
+          (rc = mpc_resident_adjoint(c, c->d_Ftab + n0, dt, len, a->segX, a->segY, a->segN,
+                                     a->lam, a->fbar + n0, (long long)n)))
+        return rc;
+      continue;
+    }
     // recompute the segment, keeping states, stage inputs and norms
     CK(cudaMemcpyAsync(a->segX, a->ckpts + n * seg, sizeof(double2) * n, cudaMemcpyDeviceToDevice,
                        c->stream));

@@ -112,6 +112,14 @@ void mpc_badj_invalidate(mpc_ctx* c);  // a setting changed: backward needs a ne
 // batched path has been tuned, else the default (batch.cu).
 int mpc_batch_variant(mpc_ctx* c, int ncol);
 int mpc_resident_run(mpc_ctx* c, double dt, int steps, int pop_index);
+bool mpc_use_resident(mpc_ctx* c);  // the resident path applies (set-up done, not disabled)
+bool mpc_resident_adjoint_ok(mpc_ctx* c);
+int mpc_resident_forward_ex(mpc_ctx* c, const double2* x_in, double2* x_out, const double* Ftab,
+                            double dt, int steps, double2* seg_x, double2* seg_y,
+                            double* norm_hist, double2* ckpt, int ckpt_every, long long vpitch);
+int mpc_resident_adjoint(mpc_ctx* c, const double* Ftab, double dt, int len,
+                         const double2* seg_x, const double2* seg_y, const double* seg_n,
+                         double2* lam, double* fbar, long long vpitch);
 
 // Launch helpers of the single-pulse path (mpc_tdse.cu), used by adjoint.cu.
 int mpc_launch_stream(mpc_ctx* c, const double2* y);

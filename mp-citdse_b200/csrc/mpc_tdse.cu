@@ -408,6 +408,8 @@ int mpc_fill_field_table(mpc_ctx* c, const double* F, int steps) {
   return MPC_OK;
 }
 
+bool mpc_use_resident(mpc_ctx* c) { return use_resident(c); }
+
 extern "C" {
 
 int mpc_version(void) { return 100; }

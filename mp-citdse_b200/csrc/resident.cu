@@ -58,28 +58,36 @@ struct ResArgs {
   int gauge;               // 0 length, 1 velocity
   int first_is_normalised; // XN at entry holds a normalised x (norm 1)
   double dt;
+  // optional outputs of the adjoint's passes (null when unused); slots are
+  // vpitch complex apart
+  double2* seg_x;          // x_n at the start of every step (normalised)
+  double2* seg_y;          // stage inputs: slot step*13 + s holds y_s, s = 1..12
+  double2* ckpt;           // x every ckpt_every steps: slot k holds x after k*ckpt_every
+  int ckpt_every;
+  long long vpitch;
   Geometry g;
 };
 
 // Grid barrier on a counter and a generation word; bounded wait.  Returns
 // false if it timed out (status raised).
-__device__ bool grid_sync(const ResArgs& a, unsigned& gen, bool& dead) {
+__device__ bool bar_sync(unsigned* count, unsigned* genw, unsigned* status, unsigned& gen,
+                         bool& dead) {
   __syncthreads();
   __shared__ int timed_out;
   if (threadIdx.x == 0) {
     timed_out = 0;
     __threadfence();
     const unsigned g0 = gen;
-    if (atomicAdd(a.bar_count, 1u) == gridDim.x - 1) {
-      atomicExch(a.bar_count, 0u);
+    if (atomicAdd(count, 1u) == gridDim.x - 1) {
+      atomicExch(count, 0u);
       __threadfence();
-      atomicAdd(a.bar_gen, 1u);
+      atomicAdd(genw, 1u);
     } else {
       const unsigned long long t0 = globaltimer_ns();
       unsigned it = 0;
-      while (*(volatile unsigned*)a.bar_gen == g0) {
+      while (*(volatile unsigned*)genw == g0) {
         if ((++it & 1023u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) {
-          atomicOr(a.status, ST_WAIT_TIMEOUT);
+          atomicOr(status, ST_WAIT_TIMEOUT);
           timed_out = 1;
           break;
         }
@@ -93,37 +101,27 @@ __device__ bool grid_sync(const ResArgs& a, unsigned& gen, bool& dead) {
   return !dead;
 }
 
+__device__ bool grid_sync(const ResArgs& a, unsigned& gen, bool& dead) {
+  return bar_sync(a.bar_count, a.bar_gen, a.status, gen, dead);
+}
+
 __device__ __forceinline__ double2 ld_cg(const double2* p) { return __ldcg(p); }
 
-__global__ void __launch_bounds__(RTHREADS, 1) k_prop_resident(const __grid_constant__ ResArgs a) {
-  extern __shared__ __align__(16) unsigned char rsm[];
-  const Geometry& g = a.g;
-  const int G = gridDim.x, c = blockIdx.x;
-  const int row0 = (int)((long long)g.ntot * c / G);
-  const int row1 = (int)((long long)g.ntot * (c + 1) / G);
-  const int nrows = row1 - row0;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-  // blocks touched by this CTA's rows and the stage-vector window they couple to
+// The stage-vector window [wlo, whi) this CTA's rows [row0, row1) couple to.
+__device__ void row_window(const Geometry& g, int row0, int row1, int& wlo, int& whi) {
   int Llo = 0;
   while (Llo + 1 < g.nstate_blk && row0 >= g.state_off[Llo + 1]) ++Llo;
   int Lhi = Llo;
   while (Lhi + 1 < g.nstate_blk && row1 - 1 >= g.state_off[Lhi + 1]) ++Lhi;
-  const int wlo = g.state_off[max(Llo - 1, 0)];
-  const int whi = g.state_off[min(Lhi + 2, g.nstate_blk)];
-  const int wlen = whi - wlo;
+  wlo = g.state_off[max(Llo - 1, 0)];
+  whi = g.state_off[min(Lhi + 2, g.nstate_blk)];
+}
 
-  // shared layout: [row offsets (int, kMaxRowsPerCta+1)] [ywin (double2, wlen)]
-  // [k (double2, 13 x nrows)] [x (double2, nrows)] [coupling rows (double)]
-  int* roff = reinterpret_cast<int*>(rsm);
-  double2* ywin = reinterpret_cast<double2*>(rsm + 16 * ((4 * (kMaxRowsPerCta + 1) + 15) / 16));
-  double2* ksm = ywin + wlen;
-  double2* xsm = ksm + kNumStages * nrows;
-  double* crow = reinterpret_cast<double*>(xsm + nrows);
-  __shared__ double red[RWARPS];
-  __shared__ double nrm_sh;
-
-  // ---- load the coupling rows once ----
+// Loads, once, each row's two coupling segments: column r of D_{L-1}, then
+// row r of D_L (negated in the velocity gauge); roff[li] is row li's offset.
+__device__ void load_rows(const Geometry& g, const double* D, int gauge, int row0, int nrows,
+                          int* roff, double* crow) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     int o = 0;
     for (int li = 0; li < nrows; ++li) {
@@ -146,15 +144,78 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_prop_resident(const __grid_cons
     int o = 0;
     if (L > 0) {
       const BlockGeom& b = g.blk[L - 1];  // column r of D_{L-1}
-      for (int k = lane; k < b.nrow; k += 32) dst[k] = a.D[b.d_off + (long long)k * b.pitch + r];
+      for (int k = lane; k < b.nrow; k += 32) dst[k] = D[b.d_off + (long long)k * b.pitch + r];
       o = b.nrow;
     }
     if (L < g.nblk) {
       const BlockGeom& b = g.blk[L];      // row r of D_L
-      const double sg = (a.gauge == 1) ? -1.0 : 1.0;
-      for (int k = lane; k < b.ncol; k += 32) dst[o + k] = sg * a.D[b.d_off + (long long)r * b.pitch + k];
+      const double sg = (gauge == 1) ? -1.0 : 1.0;
+      for (int k = lane; k < b.ncol; k += 32) dst[o + k] = sg * D[b.d_off + (long long)r * b.pitch + k];
     }
   }
+}
+
+// Coupling of row i (block L) with the window: W = sum_k crow[k] y_k over the
+// coupled blocks, lanes striding k, then a fixed xor tree (all lanes hold W).
+__device__ __forceinline__ void row_coupling(const Geometry& g, const double* cr,
+                                             const double2* ywin, int wlo, int L, int lane,
+                                             double& wr, double& wi) {
+  wr = 0.0;
+  wi = 0.0;
+  int o = 0;
+  if (L > 0) {
+    const int nlo = g.state_off[L] - g.state_off[L - 1];
+    const double2* yl = ywin + (g.state_off[L - 1] - wlo);
+    for (int k = lane; k < nlo; k += 32) {
+      const double d = cr[k];
+      const double2 y = yl[k];
+      wr = fma(d, y.x, wr);
+      wi = fma(d, y.y, wi);
+    }
+    o = nlo;
+  }
+  if (L < g.nblk) {
+    const int nup = g.state_off[L + 2] - g.state_off[L + 1];
+    const double2* yu = ywin + (g.state_off[L + 1] - wlo);
+    for (int k = lane; k < nup; k += 32) {
+      const double d = cr[o + k];
+      const double2 y = yu[k];
+      wr = fma(d, y.x, wr);
+      wi = fma(d, y.y, wi);
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    wr += __shfl_xor_sync(0xffffffffu, wr, off);
+    wi += __shfl_xor_sync(0xffffffffu, wi, off);
+  }
+}
+
+__global__ void __launch_bounds__(RTHREADS, 1) k_prop_resident(const __grid_constant__ ResArgs a) {
+  extern __shared__ __align__(16) unsigned char rsm[];
+  const Geometry& g = a.g;
+  const int G = gridDim.x, c = blockIdx.x;
+  const int row0 = (int)((long long)g.ntot * c / G);
+  const int row1 = (int)((long long)g.ntot * (c + 1) / G);
+  const int nrows = row1 - row0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  // the stage-vector window this CTA's rows couple to
+  int wlo, whi;
+  row_window(g, row0, row1, wlo, whi);
+  const int wlen = whi - wlo;
+
+  // shared layout: [row offsets (int, kMaxRowsPerCta+1)] [ywin (double2, wlen)]
+  // [k (double2, 13 x nrows)] [x (double2, nrows)] [coupling rows (double)]
+  int* roff = reinterpret_cast<int*>(rsm);
+  double2* ywin = reinterpret_cast<double2*>(rsm + 16 * ((4 * (kMaxRowsPerCta + 1) + 15) / 16));
+  double2* ksm = ywin + wlen;
+  double2* xsm = ksm + kNumStages * nrows;
+  double* crow = reinterpret_cast<double*>(xsm + nrows);
+  __shared__ double red[RWARPS];
+  __shared__ double nrm_sh;
+
+  // ---- load the coupling rows once ----
+  load_rows(g, a.D, a.gauge, row0, nrows, roff, crow);
   unsigned gen = *(volatile unsigned*)a.bar_gen;
   bool dead = false;
   __syncthreads();
@@ -184,14 +245,20 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_prop_resident(const __grid_cons
           ywin[k] = divide ? make_double2(v.x / nrm, v.y / nrm) : v;
         }
         __syncthreads();
-        for (int li = threadIdx.x; li < nrows; li += RTHREADS) xsm[li] = ywin[row0 + li - wlo];
-        if (c == 0 && threadIdx.x == 0 && step > 0) a.norm_hist[step - 1] = nrm;
+        const bool to_ckpt = a.ckpt && step > 0 && step % a.ckpt_every == 0;
+        for (int li = threadIdx.x; li < nrows; li += RTHREADS) {
+          const double2 v = ywin[row0 + li - wlo];
+          xsm[li] = v;
+          if (a.seg_x) a.seg_x[a.vpitch * step + row0 + li] = v;
+          if (to_ckpt) a.ckpt[a.vpitch * (step / a.ckpt_every) + row0 + li] = v;
+        }
+        if (c == 0 && threadIdx.x == 0 && step > 0 && a.norm_hist) a.norm_hist[step - 1] = nrm;
         if (threadIdx.x == 0 && a.pop_index >= row0 && a.pop_index < row1) {
           const double2 v = ywin[a.pop_index - wlo];
           a.pop_hist[step] = __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y));
         }
       } else {
-        const double2* Yin = a.Y[s & 1];
+        const double2* Yin = a.seg_y ? a.seg_y + a.vpitch * (step * 13LL + s) : a.Y[s & 1];
         for (int k = threadIdx.x; k < wlen; k += RTHREADS) ywin[k] = ld_cg(Yin + wlo + k);
       }
       __syncthreads();
@@ -200,34 +267,8 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_prop_resident(const __grid_cons
         const int i = row0 + li;
         int L = 0;
         while (L + 1 < g.nstate_blk && i >= g.state_off[L + 1]) ++L;
-        const double* cr = crow + roff[li];
-        double wr = 0.0, wi = 0.0;
-        int o = 0;
-        if (L > 0) {
-          const int nlo = g.state_off[L] - g.state_off[L - 1];
-          const double2* yl = ywin + (g.state_off[L - 1] - wlo);
-          for (int k = lane; k < nlo; k += 32) {
-            const double d = cr[k];
-            const double2 y = yl[k];
-            wr = fma(d, y.x, wr);
-            wi = fma(d, y.y, wi);
-          }
-          o = nlo;
-        }
-        if (L < g.nblk) {
-          const int nup = g.state_off[L + 2] - g.state_off[L + 1];
-          const double2* yu = ywin + (g.state_off[L + 1] - wlo);
-          for (int k = lane; k < nup; k += 32) {
-            const double d = cr[o + k];
-            const double2 y = yu[k];
-            wr = fma(d, y.x, wr);
-            wi = fma(d, y.y, wi);
-          }
-        }
-        for (int off = 16; off > 0; off >>= 1) {
-          wr += __shfl_xor_sync(0xffffffffu, wr, off);
-          wi += __shfl_xor_sync(0xffffffffu, wi, off);
-        }
+        double wr, wi;
+        row_coupling(g, crow + roff[li], ywin, wlo, L, lane, wr, wi);
         if (lane == 0) {
           const double e = a.eps[i];
           const double2 y = ywin[i - wlo];
@@ -259,6 +300,8 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_prop_resident(const __grid_cons
         if (last) {
           a.XN[row0 + li] = acc;
           nsq += __dadd_rn(__dmul_rn(acc.x, acc.x), __dmul_rn(acc.y, acc.y));
+        } else if (a.seg_y) {
+          a.seg_y[a.vpitch * (step * 13LL + s + 1) + row0 + li] = acc;
         } else {
           a.Y[(s + 1) & 1][row0 + li] = acc;
         }
@@ -288,7 +331,7 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_prop_resident(const __grid_cons
   const double nrm = nrm_sh;
   if (a.steps > 0) {
     if (c == 0 && threadIdx.x == 0) {
-      a.norm_hist[a.steps - 1] = nrm;
+      if (a.norm_hist) a.norm_hist[a.steps - 1] = nrm;
       if (!(nrm > 0.0) || !isfinite(nrm)) atomicOr(a.status, ST_NONFINITE);
     }
     for (int li = threadIdx.x; li < nrows; li += RTHREADS) {
@@ -299,6 +342,187 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_prop_resident(const __grid_cons
         a.pop_hist[a.steps] = __dadd_rn(__dmul_rn(o.x, o.x), __dmul_rn(o.y, o.y));
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// The adjoint sweep of one checkpoint segment on the resident layout (the
+// reverse pass of the objective gradient, adjoint.cu): per step n, backwards,
+//   d = Re<x_{n+1}, lam>            (per-CTA partials, a grid barrier, then the
+//                                    same fixed-order sum in every CTA)
+//   zbar = (lam - x_{n+1} d) / ||z_n||,   kbar_12 = h b_12 zbar
+//   for s = 12 .. 0:  ybar_s = -M(F_n) kbar_s   (the coupling of kbar_s: the
+//     same shared-memory rows and window as the forward, one barrier per stage)
+//     dJ/dF_n += -Re<M1 kbar_s, y_s>
+//     kbar_{s-1} = h b_{s-1} zbar + sum_{j>=s} h a_{j,s-1} ybar_j, or after
+//     stage 0 lam_n = zbar + sum_j ybar_j.
+// lam lives in shared memory for the CTA's rows (no other CTA reads it);
+// kbar is exchanged through a ping-pong pair in global memory.
+struct AdjResArgs {
+  const double* D;
+  const double* eps;
+  const double* Ftab;      // field of local step j at Ftab[j]
+  const double2* seg_x;    // x_j, j = 0..len (normalised), vpitch apart
+  const double2* seg_y;    // y_s of step j at slot j*13 + s, s = 1..12
+  const double* seg_n;     // ||z_j||
+  double2* lam;            // in: lambda after the segment; out: before it
+  double2* kb[2];          // kbar ping-pong [ntot]
+  double* part;            // [G] partials of the inner product
+  double* fpart;           // [len][G] per-CTA dJ/dF of each step
+  unsigned* bar_count;
+  unsigned* bar_gen;
+  unsigned* status;
+  int len;
+  int gauge;
+  double dt;
+  long long vpitch;
+  Geometry g;
+};
+
+__constant__ double r_At[13][13];  // a_{j,s} at [s][j]
+
+__global__ void __launch_bounds__(RTHREADS, 1) k_adj_resident(const __grid_constant__ AdjResArgs a) {
+  extern __shared__ __align__(16) unsigned char rsm[];
+  const Geometry& g = a.g;
+  const int G = gridDim.x, c = blockIdx.x;
+  const int row0 = (int)((long long)g.ntot * c / G);
+  const int row1 = (int)((long long)g.ntot * (c + 1) / G);
+  const int nrows = row1 - row0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int wlo, whi;
+  row_window(g, row0, row1, wlo, whi);
+  const int wlen = whi - wlo;
+  // shared layout: [row offsets] [window (double2, wlen)] [ybar (double2, 13 x nrows)]
+  // [zbar (double2, nrows)] [lam (double2, nrows)] [dJ/dF per row (double, nrows)]
+  // [coupling rows (double)]
+  int* roff = reinterpret_cast<int*>(rsm);
+  double2* ywin = reinterpret_cast<double2*>(rsm + 16 * ((4 * (kMaxRowsPerCta + 1) + 15) / 16));
+  double2* ybs = ywin + wlen;
+  double2* zbs = ybs + kNumStages * nrows;
+  double2* lams = zbs + nrows;
+  double* frow = reinterpret_cast<double*>(lams + nrows);
+  double* crow = frow + ((nrows + 1) & ~1);
+  __shared__ double red[RWARPS];
+  __shared__ double d_sh;
+
+  load_rows(g, a.D, a.gauge, row0, nrows, roff, crow);
+  for (int li = threadIdx.x; li < nrows; li += RTHREADS) lams[li] = ld_cg(a.lam + row0 + li);
+  unsigned gen = *(volatile unsigned*)a.bar_gen;
+  bool dead = false;
+  __syncthreads();
+
+  const double h = a.dt;
+  const long long vp = a.vpitch;
+  for (int j = a.len - 1; j >= 0 && !dead; --j) {
+    const double F = a.Ftab[j];
+    const double2* x1 = a.seg_x + vp * (j + 1);
+    // ---- d = Re<x_{n+1}, lam> ----
+    double v = 0.0;
+    for (int li = threadIdx.x; li < nrows; li += RTHREADS) {
+      const double2 x = ld_cg(x1 + row0 + li), l = lams[li];
+      v += __dadd_rn(__dmul_rn(x.x, l.x), __dmul_rn(x.y, l.y));
+    }
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = red[0];
+      for (int w = 1; w < RWARPS; ++w) t += red[w];
+      a.part[c] = t;
+    }
+    if (!bar_sync(a.bar_count, a.bar_gen, a.status, gen, dead)) break;
+    if (threadIdx.x < 32) {
+      double t = 0.0;
+      for (int p = threadIdx.x; p < G; p += 32) t += __ldcg(a.part + p);
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (threadIdx.x == 0) d_sh = t;
+    }
+    __syncthreads();
+    // ---- zbar and kbar_12 ----
+    {
+      const double d = d_sh, nz = __ldcg(a.seg_n + j), hb = h * r_B8[kNumStages - 1];
+      for (int li = threadIdx.x; li < nrows; li += RTHREADS) {
+        const double2 l = lams[li], x = ld_cg(x1 + row0 + li);
+        const double2 z = make_double2((l.x - x.x * d) / nz, (l.y - x.y * d) / nz);
+        zbs[li] = z;
+        a.kb[0][row0 + li] = make_double2(hb * z.x, hb * z.y);
+        frow[li] = 0.0;
+      }
+    }
+    if (!bar_sync(a.bar_count, a.bar_gen, a.status, gen, dead)) break;
+    double fcta = 0.0;
+    for (int s = kNumStages - 1; s >= 0; --s) {
+      const double2* kin = a.kb[s & 1];
+      for (int k = threadIdx.x; k < wlen; k += RTHREADS) ywin[k] = ld_cg(kin + wlo + k);
+      __syncthreads();
+      for (int li = warp; li < nrows; li += RWARPS) {
+        const int i = row0 + li;
+        int L = 0;
+        while (L + 1 < g.nstate_blk && i >= g.state_off[L + 1]) ++L;
+        double wr, wi;
+        row_coupling(g, crow + roff[li], ywin, wlo, L, lane, wr, wi);
+        if (lane == 0) {
+          const double e = a.eps[i];
+          const double2 kv = ywin[i - wlo];
+          // M1 kbar: -i W (length) or W (velocity, signs in the rows)
+          const double2 m1 = (a.gauge == 0) ? make_double2(wi, -wr) : make_double2(wr, wi);
+          // ybar_s = -M kbar = -(-i e kbar + F M1 kbar)
+          const double2 yb = make_double2(-(__dmul_rn(e, kv.y) + __dmul_rn(F, m1.x)),
+                                          -(__dmul_rn(-e, kv.x) + __dmul_rn(F, m1.y)));
+          ybs[s * nrows + li] = yb;
+          const double2 y = (s == 0) ? ld_cg(a.seg_x + vp * j + i)
+                                     : ld_cg(a.seg_y + vp * (j * 13LL + s) + i);
+          frow[li] = -(__dmul_rn(m1.x, y.x) + __dmul_rn(m1.y, y.y));
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {  // this stage's dJ/dF, rows in order
+        double t = 0.0;
+        for (int li = 0; li < nrows; ++li) t += frow[li];
+        fcta += t;
+      }
+      double2* kout = a.kb[(s + 1) & 1];
+      for (int li = threadIdx.x; li < nrows; li += RTHREADS) {
+        if (s > 0) {
+          const double cb = h * r_B8[s - 1];
+          const double2 z = zbs[li];
+          double2 o = make_double2(__dmul_rn(cb, z.x), __dmul_rn(cb, z.y));
+          for (int sp = s; sp < kNumStages; ++sp) {
+            const double cf = r_At[s - 1][sp];
+            if (cf == 0.0) continue;
+            const double2 w = ybs[sp * nrows + li];
+            const double cc = h * cf;
+            o.x = __dadd_rn(o.x, __dmul_rn(cc, w.x));
+            o.y = __dadd_rn(o.y, __dmul_rn(cc, w.y));
+          }
+          kout[row0 + li] = o;
+        } else {
+          double2 o = zbs[li];
+          for (int sp = 0; sp < kNumStages; ++sp) {
+            const double2 w = ybs[sp * nrows + li];
+            o.x = __dadd_rn(o.x, w.x);
+            o.y = __dadd_rn(o.y, w.y);
+          }
+          lams[li] = o;
+        }
+      }
+      if (s > 0 && !bar_sync(a.bar_count, a.bar_gen, a.status, gen, dead)) break;
+      __syncthreads();
+    }
+    if (dead) break;
+    if (threadIdx.x == 0) a.fpart[(long long)j * G + c] = fcta;
+  }
+  if (dead) return;
+  __syncthreads();
+  for (int li = threadIdx.x; li < nrows; li += RTHREADS) a.lam[row0 + li] = lams[li];
+}
+
+// dJ/dF_n = sum over CTAs of the step's partials, in CTA order.
+__global__ void k_adj_res_fbar(const double* fpart, int len, int G, double* fbar) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= len) return;
+  double t = 0.0;
+  for (int p = 0; p < G; ++p) t += fpart[(long long)j * G + p];
+  fbar[j] = t;
 }
 
 size_t resident_smem(const Geometry& g, int G, int* max_rows) {
@@ -333,6 +557,11 @@ size_t resident_smem(const Geometry& g, int G, int* max_rows) {
 struct mpc_resident_state {
   int G = 0;
   size_t smem = 0;
+  size_t smem_adj = 0;
+  bool adj_ok = false;      // the adjoint sweep kernel fits as well
+  double2* kb = nullptr;    // [2][ntot] kbar ping-pong of the adjoint sweep
+  double* fpart = nullptr;  // [fpart_cap][G]
+  int fpart_cap = 0;
   double2* Y0 = nullptr;
   double2* Y1 = nullptr;
   double2* XN = nullptr;
@@ -369,9 +598,26 @@ bool mpc_resident_setup(mpc_ctx* c) {
     B8[i] = rkf78::B8[i];
     for (int j = 0; j < 13; ++j) A[i][j] = rkf78::A[i][j];
   }
+  double At[13][13];
+  for (int i = 0; i < 13; ++i)
+    for (int j = 0; j < 13; ++j) At[i][j] = rkf78::A[j][i];
   if (cudaMemcpyToSymbol(r_A, A, sizeof A) != cudaSuccess ||
-      cudaMemcpyToSymbol(r_B8, B8, sizeof B8) != cudaSuccess)
+      cudaMemcpyToSymbol(r_B8, B8, sizeof B8) != cudaSuccess ||
+      cudaMemcpyToSymbol(r_At, At, sizeof At) != cudaSuccess)
     return false;
+  // the adjoint sweep: two more vectors and a double per row
+  const size_t smem_adj = smem + 24 * (size_t)max_rows + 16;
+  int per_sm_adj = 0;
+  if (smem_adj + 2048 <= (size_t)optin &&
+      cudaFuncSetAttribute(k_adj_resident, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem_adj) == cudaSuccess &&
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_adj, k_adj_resident, RTHREADS,
+                                                    smem_adj) == cudaSuccess &&
+      per_sm_adj >= 1) {
+    r->smem_adj = smem_adj;
+    r->adj_ok = true;
+  }
+  cudaGetLastError();
   const size_t n = c->g.ntot;
   if (cudaMalloc(&r->Y0, sizeof(double2) * n) != cudaSuccess ||
       cudaMalloc(&r->Y1, sizeof(double2) * n) != cudaSuccess ||
@@ -391,6 +637,8 @@ bool mpc_resident_setup(mpc_ctx* c) {
 void mpc_resident_free(mpc_ctx* c) {
   if (!c || !c->resident) return;
   mpc_resident_state* r = c->resident;
+  cudaFree(r->kb);
+  cudaFree(r->fpart);
   cudaFree(r->Y0);
   cudaFree(r->Y1);
   cudaFree(r->XN);
@@ -431,5 +679,99 @@ int mpc_resident_run(mpc_ctx* c, double dt, int steps, int pop_index) {
   ProfScope ps(c, MPC_KERNEL_RESIDENT);
   CK(cudaLaunchCooperativeKernel((const void*)k_prop_resident, dim3(r->G), dim3(RTHREADS), args,
                                  r->smem, c->stream));
+  return MPC_OK;
+}
+
+// The fixed-step loop from x_in (device, normalised or as given) for `steps`
+// steps with the field table Ftab, result (normalised) into x_out; optional
+// outputs for the objective gradient: seg_x / seg_y / norm_hist (every step's
+// state, stage inputs and norm) and ckpt (the state every ckpt_every steps),
+// slots vpitch complex apart.
+int mpc_resident_forward_ex(mpc_ctx* c, const double2* x_in, double2* x_out, const double* Ftab,
+                            double dt, int steps, double2* seg_x, double2* seg_y,
+                            double* norm_hist, double2* ckpt, int ckpt_every, long long vpitch) {
+  mpc_resident_state* r = c->resident;
+  ResArgs a{};
+  a.D = c->d_D;
+  a.eps = c->d_eps;
+  a.Ftab = Ftab;
+  a.Y[0] = r->Y0;
+  a.Y[1] = r->Y1;
+  a.XN = r->XN;
+  a.xout = x_out;
+  a.norm_part = r->part;
+  a.bar_count = r->bar;
+  a.bar_gen = r->bar + 1;
+  a.status = c->d_status;
+  a.pop_hist = nullptr;
+  a.norm_hist = norm_hist;
+  a.pop_index = -1;
+  a.steps = steps;
+  a.gauge = (c->gauge == 'l') ? 0 : 1;
+  a.first_is_normalised = 1;
+  a.dt = dt;
+  a.seg_x = seg_x;
+  a.seg_y = seg_y;
+  a.ckpt = ckpt;
+  a.ckpt_every = ckpt_every > 0 ? ckpt_every : 1;
+  a.vpitch = vpitch;
+  a.g = c->g;
+  CK(cudaMemcpyAsync(r->XN, x_in, sizeof(double2) * c->g.ntot, cudaMemcpyDeviceToDevice,
+                     c->stream));
+  CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned), c->stream));
+  void* args[] = {&a};
+  ProfScope ps(c, MPC_KERNEL_RESIDENT);
+  CK(cudaLaunchCooperativeKernel((const void*)k_prop_resident, dim3(r->G), dim3(RTHREADS), args,
+                                 r->smem, c->stream));
+  ++c->launches;
+  return MPC_OK;
+}
+
+bool mpc_resident_adjoint_ok(mpc_ctx* c) { return c->resident && c->resident->adj_ok; }
+
+// The adjoint sweep of one segment of len steps (see k_adj_resident); lam in
+// and out (device, ntot), dJ/dF of the segment's steps into fbar [len].
+int mpc_resident_adjoint(mpc_ctx* c, const double* Ftab, double dt, int len,
+                         const double2* seg_x, const double2* seg_y, const double* seg_n,
+                         double2* lam, double* fbar, long long vpitch) {
+  mpc_resident_state* r = c->resident;
+  if (!r || !r->adj_ok) return mpc_fail(MPC_ERR_ARG, "resident adjoint unavailable");
+  if (!r->kb) CK(cudaMalloc(&r->kb, sizeof(double2) * 2 * (size_t)c->g.ntot));
+  if (r->fpart_cap < len) {
+    cudaFree(r->fpart);
+    r->fpart = nullptr;
+    CK(cudaMalloc(&r->fpart, sizeof(double) * (size_t)len * r->G));
+    r->fpart_cap = len;
+  }
+  AdjResArgs a{};
+  a.D = c->d_D;
+  a.eps = c->d_eps;
+  a.Ftab = Ftab;
+  a.seg_x = seg_x;
+  a.seg_y = seg_y;
+  a.seg_n = seg_n;
+  a.lam = lam;
+  a.kb[0] = r->kb;
+  a.kb[1] = r->kb + c->g.ntot;
+  a.part = r->part;
+  a.fpart = r->fpart;
+  a.bar_count = r->bar;
+  a.bar_gen = r->bar + 1;
+  a.status = c->d_status;
+  a.len = len;
+  a.gauge = (c->gauge == 'l') ? 0 : 1;
+  a.dt = dt;
+  a.vpitch = vpitch;
+  a.g = c->g;
+  CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned), c->stream));
+  void* args[] = {&a};
+  {
+    ProfScope ps(c, MPC_KERNEL_RESIDENT);
+    CK(cudaLaunchCooperativeKernel((const void*)k_adj_resident, dim3(r->G), dim3(RTHREADS), args,
+                                   r->smem_adj, c->stream));
+  }
+  k_adj_res_fbar<<<(len + 127) / 128, 128, 0, c->stream>>>(r->fpart, len, r->G, fbar);
+  CK(cudaGetLastError());
+  c->launches += 2;
   return MPC_OK;
 }
