@@ -27,14 +27,18 @@ def _problem(g, seed=0, n_per_l=30, l_max=3, steps=400, K=48):
     return s, p, u, steps * 0.1, x0, steps
 
 
+@pytest.mark.parametrize("path", ["auto", "streaming"])
 @pytest.mark.parametrize("g", ["l", "v"])
 @pytest.mark.parametrize("target", [-1, 5])
-def test_adjoint_matches_oracle(oracle, g, target):
+def test_adjoint_matches_oracle(oracle, g, target, path):
+    """Both implementations: the persistent resident passes (auto, the
+    couplings fit in shared memory) and the streamed step-by-step kernels."""
     s, p, u, T, x0, steps = _problem(g)
     kind = "sineEE" if g == "l" else "sineAA"
     Jo, go, fbo, _ = oracle.objective_gradient(s.n, s.eig, s.dip, g, kind, p.as_array(), u, T,
                                                0.0, 0.1, steps, x0, target)
     with mpc_tdse.Context.from_system(s) as ctx:
+        ctx.set_path(path)
         J, gr, fb = ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0, target, ckpt_every=64)
     assert abs(J - Jo) < 1e-12
     assert np.max(np.abs(fb - fbo)) <= 1e-9 * np.max(np.abs(fbo))
@@ -55,9 +59,11 @@ def test_adjoint_matches_central_differences():
             assert abs(fd - gr[k]) <= 1e-6 * max(abs(fd), 1e-8 * np.max(np.abs(gr))), (k, fd, gr[k])
 
 
-def test_checkpoint_interval_does_not_change_the_gradient():
+@pytest.mark.parametrize("path", ["auto", "streaming"])
+def test_checkpoint_interval_does_not_change_the_gradient(path):
     s, p, u, T, x0, steps = _problem("v", seed=4, steps=301)
     with mpc_tdse.Context.from_system(s) as ctx:
+        ctx.set_path(path)
         J1, g1, f1 = ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0, -1, ckpt_every=64)
         J2, g2, f2 = ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0, -1, ckpt_every=7)
         J3, g3, f3 = ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0, -1, ckpt_every=1000)
@@ -128,3 +134,17 @@ def test_2e_ionisation_yields_match_oracle_and_differences(oracle, thr):
     assert abs(J - Jo) < 1e-12
     assert np.max(np.abs(gr - go)) <= 1e-9 * np.max(np.abs(go))
     assert abs(fd - gr[k]) <= 1e-6 * max(abs(fd), 1e-8 * np.max(np.abs(gr)))
+
+
+def test_resident_and_streamed_adjoints_agree():
+    s, p, u, T, x0, steps = _problem("l", seed=8, steps=200)
+    out = {}
+    for path in ("auto", "streaming"):
+        with mpc_tdse.Context.from_system(s) as ctx:
+            ctx.set_path(path)
+            assert ctx.path == ("resident" if path == "auto" else "streaming")
+            out[path] = ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0, -1, ckpt_every=16)
+    (J1, g1, f1), (J2, g2, f2) = out["auto"], out["streaming"]
+    assert abs(J1 - J2) < 1e-14
+    assert np.max(np.abs(g1 - g2)) <= 1e-12 * np.max(np.abs(g2))
+    assert np.max(np.abs(f1 - f2)) <= 1e-12 * np.max(np.abs(f2))
