@@ -67,7 +67,7 @@ struct BrArgs {
   const CtaPart* part;
   double* red_nrm;    // [G][kMaxP]
   double* red_err;    // [G][kMaxP]
-  unsigned* bar;      // [0] arrival count, [1] generation
+  unsigned* bar;      // 64-bit arrival counter (two words), cleared per launch
   unsigned* status;
   int ldc, ncol, ntot;
   int exit_below, max_attempts, gauge;
@@ -75,29 +75,27 @@ struct BrArgs {
   Geometry g;
 };
 
-// Grid barrier with a bounded wait: returns false (status raised) on timeout.
-__device__ bool br_sync(const BrArgs& a, unsigned& gen, int* s_dead) {
+// Grid barrier on a monotonic 64-bit arrival counter (cleared before each
+// launch): the CTA's e-th barrier completes when the counter reaches
+// e * gridDim.x.  Bounded wait: returns false (status raised) on timeout.
+__device__ bool br_sync(const BrArgs& a, unsigned long long& epoch, int* s_dead) {
   __syncthreads();
   if (threadIdx.x == 0) {
+    unsigned long long* ctr = reinterpret_cast<unsigned long long*>(a.bar);
+    const unsigned long long target = (epoch + 1) * gridDim.x;
     __threadfence();
-    const unsigned g0 = gen;
-    if (atomicAdd(a.bar, 1u) == gridDim.x - 1) {
-      atomicExch(a.bar, 0u);
-      __threadfence();
-      atomicAdd(a.bar + 1, 1u);
-    } else {
-      const unsigned long long t0 = globaltimer_ns();
-      unsigned it = 0;
-      while (*(volatile unsigned*)(a.bar + 1) == g0) {
-        if ((++it & 1023u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) {
-          atomicOr(a.status, ST_WAIT_TIMEOUT);
-          *s_dead = 1;
-          break;
-        }
+    atomicAdd(ctr, 1ull);
+    const unsigned long long t0 = globaltimer_ns();
+    unsigned it = 0;
+    while (*(volatile unsigned long long*)ctr < target) {
+      if ((++it & 1023u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) {
+        atomicOr(a.status, ST_WAIT_TIMEOUT);
+        *s_dead = 1;
+        break;
       }
     }
     __threadfence();
-    gen = g0 + 1;
+    epoch += 1;
   }
   __syncthreads();
   return *s_dead == 0;
@@ -200,7 +198,7 @@ __global__ void __launch_bounds__(QT, 1) k_batch_res(const __grid_constant__ BrA
     const int li = e / P, q = e % P;
     xsm[e] = q < ncol ? __ldcg(a.X + (long long)(row0 + li) * ldc + q) : make_double2(0.0, 0.0);
   }
-  unsigned gen = *(volatile unsigned*)(a.bar + 1);
+  unsigned long long epoch = 0;
   __syncthreads();
 
   const int qc = tid % P;           // this thread's column in the coupling loop
@@ -385,7 +383,7 @@ __global__ void __launch_bounds__(QT, 1) k_batch_res(const __grid_constant__ BrA
         a.red_nrm[cta * kMaxP + tid] = ns;
         a.red_err[cta * kMaxP + tid] = em;
       }
-      if (!br_sync(a, gen, &s_dead)) break;
+      if (!br_sync(a, epoch, &s_dead)) break;
     }
     if (s_dead) break;
 
@@ -654,7 +652,7 @@ int mpc_batch_res_run(mpc_ctx* c, const BatchResLaunch& l, int P, int exit_below
   a.atol = l.atol;
   a.dt_max = l.dt_max;
   a.g = c->g;
-  CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned), c->stream));  // arrival count
+  CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned) * 2, c->stream));  // arrival counter
   void* args[] = {&a};
   ProfScope ps(c, MPC_KERNEL_RESIDENT);
   CK(cudaLaunchCooperativeKernel(br_kernel_for(P), dim3(r->G), dim3(QT), args, r->smem[P],

@@ -48,8 +48,7 @@ struct ResArgs {
   double2* XN;             // x_new (unnormalised) after each step; x at entry
   double2* xout;           // normalised state at the end
   double* norm_part;       // [G]
-  unsigned* bar_count;
-  unsigned* bar_gen;
+  unsigned* bar;           // 64-bit arrival counter (two words), cleared per launch
   unsigned* status;
   double* pop_hist;        // [steps+1] (entry 0 written too)
   double* norm_hist;       // [steps]
@@ -68,41 +67,39 @@ struct ResArgs {
   Geometry g;
 };
 
-// Grid barrier on a counter and a generation word; bounded wait.  Returns
-// false if it timed out (status raised).
-__device__ bool bar_sync(unsigned* count, unsigned* genw, unsigned* status, unsigned& gen,
-                         bool& dead) {
+// Grid barrier on a monotonic 64-bit arrival counter (cleared before each
+// launch): the CTA's e-th barrier completes when the counter reaches
+// e * gridDim.x, so the last arrival releases everyone with its one atomic
+// (no reset, no second word).  Bounded wait; returns false (status raised) if
+// it timed out.
+__device__ bool bar_sync(unsigned* bar, unsigned* status, unsigned long long& epoch, bool& dead) {
   __syncthreads();
   __shared__ int timed_out;
   if (threadIdx.x == 0) {
     timed_out = 0;
+    unsigned long long* ctr = reinterpret_cast<unsigned long long*>(bar);
+    const unsigned long long target = (epoch + 1) * gridDim.x;
     __threadfence();
-    const unsigned g0 = gen;
-    if (atomicAdd(count, 1u) == gridDim.x - 1) {
-      atomicExch(count, 0u);
-      __threadfence();
-      atomicAdd(genw, 1u);
-    } else {
-      const unsigned long long t0 = globaltimer_ns();
-      unsigned it = 0;
-      while (*(volatile unsigned*)genw == g0) {
-        if ((++it & 1023u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) {
-          atomicOr(status, ST_WAIT_TIMEOUT);
-          timed_out = 1;
-          break;
-        }
+    atomicAdd(ctr, 1ull);
+    const unsigned long long t0 = globaltimer_ns();
+    unsigned it = 0;
+    while (*(volatile unsigned long long*)ctr < target) {
+      if ((++it & 1023u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) {
+        atomicOr(status, ST_WAIT_TIMEOUT);
+        timed_out = 1;
+        break;
       }
     }
     __threadfence();
-    gen = g0 + 1;
+    epoch += 1;
   }
   __syncthreads();
   if (timed_out) dead = true;
   return !dead;
 }
 
-__device__ bool grid_sync(const ResArgs& a, unsigned& gen, bool& dead) {
-  return bar_sync(a.bar_count, a.bar_gen, a.status, gen, dead);
+__device__ bool grid_sync(const ResArgs& a, unsigned long long& epoch, bool& dead) {
+  return bar_sync(a.bar, a.status, epoch, dead);
 }
 
 __device__ __forceinline__ double2 ld_cg(const double2* p) { return __ldcg(p); }
@@ -216,7 +213,7 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_prop_resident(const __grid_cons
 
   // ---- load the coupling rows once ----
   load_rows(g, a.D, a.gauge, row0, nrows, roff, crow);
-  unsigned gen = *(volatile unsigned*)a.bar_gen;
+  unsigned long long epoch = 0;
   bool dead = false;
   __syncthreads();
 
@@ -316,7 +313,7 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_prop_resident(const __grid_cons
           a.norm_part[c] = t;
         }
       }
-      if (!grid_sync(a, gen, dead)) break;
+      if (!grid_sync(a, epoch, dead)) break;
     }
   }
   if (dead) return;
@@ -368,8 +365,7 @@ struct AdjResArgs {
   double2* kb[2];          // kbar ping-pong [ntot]
   double* part;            // [G] partials of the inner product
   double* fpart;           // [len][G] per-CTA dJ/dF of each step
-  unsigned* bar_count;
-  unsigned* bar_gen;
+  unsigned* bar;           // 64-bit arrival counter (two words), cleared per launch
   unsigned* status;
   int len;
   int gauge;
@@ -406,7 +402,7 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_adj_resident(const __grid_const
 
   load_rows(g, a.D, a.gauge, row0, nrows, roff, crow);
   for (int li = threadIdx.x; li < nrows; li += RTHREADS) lams[li] = ld_cg(a.lam + row0 + li);
-  unsigned gen = *(volatile unsigned*)a.bar_gen;
+  unsigned long long epoch = 0;
   bool dead = false;
   __syncthreads();
 
@@ -429,7 +425,7 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_adj_resident(const __grid_const
       for (int w = 1; w < RWARPS; ++w) t += red[w];
       a.part[c] = t;
     }
-    if (!bar_sync(a.bar_count, a.bar_gen, a.status, gen, dead)) break;
+    if (!bar_sync(a.bar, a.status, epoch, dead)) break;
     if (threadIdx.x < 32) {
       double t = 0.0;
       for (int p = threadIdx.x; p < G; p += 32) t += __ldcg(a.part + p);
@@ -448,7 +444,7 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_adj_resident(const __grid_const
         frow[li] = 0.0;
       }
     }
-    if (!bar_sync(a.bar_count, a.bar_gen, a.status, gen, dead)) break;
+    if (!bar_sync(a.bar, a.status, epoch, dead)) break;
     double fcta = 0.0;
     for (int s = kNumStages - 1; s >= 0; --s) {
       const double2* kin = a.kb[s & 1];
@@ -505,7 +501,7 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_adj_resident(const __grid_const
           lams[li] = o;
         }
       }
-      if (s > 0 && !bar_sync(a.bar_count, a.bar_gen, a.status, gen, dead)) break;
+      if (s > 0 && !bar_sync(a.bar, a.status, epoch, dead)) break;
       __syncthreads();
     }
     if (dead) break;
@@ -566,7 +562,7 @@ struct mpc_resident_state {
   double2* Y1 = nullptr;
   double2* XN = nullptr;
   double* part = nullptr;
-  unsigned* bar = nullptr;  // [0] count, [1] generation
+  unsigned* bar = nullptr;  // 64-bit arrival counter
   bool ok = false;
 };
 
@@ -661,8 +657,7 @@ int mpc_resident_run(mpc_ctx* c, double dt, int steps, int pop_index) {
   a.XN = r->XN;
   a.xout = c->d_x;
   a.norm_part = r->part;
-  a.bar_count = r->bar;
-  a.bar_gen = r->bar + 1;
+  a.bar = r->bar;
   a.status = c->d_status;
   a.pop_hist = c->d_pop;
   a.norm_hist = c->d_nrm;
@@ -674,7 +669,7 @@ int mpc_resident_run(mpc_ctx* c, double dt, int steps, int pop_index) {
   a.g = c->g;
   CK(cudaMemcpyAsync(r->XN, c->d_x, sizeof(double2) * c->g.ntot, cudaMemcpyDeviceToDevice,
                      c->stream));
-  CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned), c->stream));  // arrival count
+  CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned) * 2, c->stream));  // arrival counter
   void* args[] = {&a};
   ProfScope ps(c, MPC_KERNEL_RESIDENT);
   CK(cudaLaunchCooperativeKernel((const void*)k_prop_resident, dim3(r->G), dim3(RTHREADS), args,
@@ -700,8 +695,7 @@ int mpc_resident_forward_ex(mpc_ctx* c, const double2* x_in, double2* x_out, con
   a.XN = r->XN;
   a.xout = x_out;
   a.norm_part = r->part;
-  a.bar_count = r->bar;
-  a.bar_gen = r->bar + 1;
+  a.bar = r->bar;
   a.status = c->d_status;
   a.pop_hist = nullptr;
   a.norm_hist = norm_hist;
@@ -718,7 +712,7 @@ int mpc_resident_forward_ex(mpc_ctx* c, const double2* x_in, double2* x_out, con
   a.g = c->g;
   CK(cudaMemcpyAsync(r->XN, x_in, sizeof(double2) * c->g.ntot, cudaMemcpyDeviceToDevice,
                      c->stream));
-  CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned), c->stream));
+  CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned) * 2, c->stream));
   void* args[] = {&a};
   ProfScope ps(c, MPC_KERNEL_RESIDENT);
   CK(cudaLaunchCooperativeKernel((const void*)k_prop_resident, dim3(r->G), dim3(RTHREADS), args,
@@ -755,15 +749,14 @@ int mpc_resident_adjoint(mpc_ctx* c, const double* Ftab, double dt, int len,
   a.kb[1] = r->kb + c->g.ntot;
   a.part = r->part;
   a.fpart = r->fpart;
-  a.bar_count = r->bar;
-  a.bar_gen = r->bar + 1;
+  a.bar = r->bar;
   a.status = c->d_status;
   a.len = len;
   a.gauge = (c->gauge == 'l') ? 0 : 1;
   a.dt = dt;
   a.vpitch = vpitch;
   a.g = c->g;
-  CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned), c->stream));
+  CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned) * 2, c->stream));
   void* args[] = {&a};
   {
     ProfScope ps(c, MPC_KERNEL_RESIDENT);
