@@ -308,8 +308,9 @@ int aalloc(mpc_adjoint_state* a, T** p, size_t count) {
 }
 
 int ensure_adjoint(mpc_ctx* c, int steps, int ckpt) {
-  static bool consts = false;
-  if (!consts) {
+  static bool consts[64] = {};  // per device: the transposed tableau in constant memory
+  if (c->device < 0 || c->device >= 64) return mpc_fail(MPC_ERR_ARG, "device %d", c->device);
+  if (!consts[c->device]) {
     double At[13][13], b8[13];
     for (int s = 0; s < 13; ++s) {
       b8[s] = rkf78::B8[s];
@@ -317,7 +318,7 @@ int ensure_adjoint(mpc_ctx* c, int steps, int ckpt) {
     }
     CK(cudaMemcpyToSymbol(c_At, At, sizeof At));
     CK(cudaMemcpyToSymbol(c_b8, b8, sizeof b8));
-    consts = true;
+    consts[c->device] = true;
   }
   const int nseg = (steps + ckpt - 1) / ckpt;
   const size_t n = c->g.ntot + kVecPad;

@@ -83,7 +83,7 @@ __device__ bool br_sync(const BrArgs& a, unsigned long long& epoch, int* s_dead)
   if (threadIdx.x == 0) {
     unsigned long long* ctr = reinterpret_cast<unsigned long long*>(a.bar);
     const unsigned long long target = (epoch + 1) * gridDim.x;
-    __threadfence();
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");  // this CTA's writes before the arrival
     atomicAdd(ctr, 1ull);
     const unsigned long long t0 = globaltimer_ns();
     unsigned it = 0;
@@ -94,7 +94,7 @@ __device__ bool br_sync(const BrArgs& a, unsigned long long& epoch, int* s_dead)
         break;
       }
     }
-    __threadfence();
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");  // others' writes after the wait
     epoch += 1;
   }
   __syncthreads();
