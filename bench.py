@@ -259,6 +259,29 @@ def batched_kernel_case(local):
           f"resident 4 pulses: {int(acc4.sum() + rej4.sum())} pulse-attempts")
 
 
+def adjoint_kernel_case(local):
+    """A short gradient for profilers: the adjoint workload's system, pulse
+    and 4096 controls over the first 256 steps, checkpoint every 64 (one
+    resident forward launch, then per segment a resident recompute and a
+    resident adjoint sweep)."""
+    import numpy as np
+
+    import mpc_tdse
+    from mpc_tdse.structure1e import hydrogen
+
+    s = hydrogen(n=400, k=9, R=200.0, l_max=8, gauge="l", states=[388] * 9)
+    ctx = mpc_tdse.Context.from_system(s, device=local)
+    Io, w = mpc_tdse.to_au(1e14, 1.5498)
+    tau = mpc_tdse.period(w, 10)
+    p = mpc_tdse.pulse_setup("sine", "l", Io, w, 0.0, 10, tau)
+    u = np.random.default_rng(1).standard_normal(4096) * 0.01 * p.Eo
+    x0 = np.zeros(s.ntot, complex)
+    x0[0] = 1.0
+    J, g, _ = ctx.objective_gradient(p, u, tau, 0.0, 0.05, 256, x0, -1, 64)
+    ctx.close()
+    print(f"adjoint 256 steps on {s.ntot} states: J = {J:.6e}, |dJ/du| = {np.linalg.norm(g):.3e}")
+
+
 def measure_adjoint(local, stream_cls, n_fd=2):
     """Adjoint gradient of the ionisation yield w.r.t. 4096 E(t) control
     samples: 1e H-like, 398 states/l, l = 0..8 (3582 states), length gauge,
@@ -525,11 +548,13 @@ def main():
                     help="skip the adjoint-gradient measurement")
     ap.add_argument("--no-he2e-batched", action="store_true",
                     help="skip the batched + adjoint 2e measurement (30k states, 64 pulses)")
-    ap.add_argument("--mode", default="full", choices=["full", "kernel", "batched-kernel"],
+    ap.add_argument("--mode", default="full",
+                    choices=["full", "kernel", "batched-kernel", "adjoint-kernel"],
                     help="kernel: only warm-up + timed steps of the workload (a small case for "
                          "profilers); batched-kernel: a short batched run (256 pulses at full "
-                         "width, then 4 pulses in the resident kernel) for profilers; no JSON "
-                         "line")
+                         "width, then 4 pulses in the resident kernel) for profilers; "
+                         "adjoint-kernel: one objective gradient of the adjoint workload over "
+                         "its first 256 steps (resident passes); no JSON line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -541,6 +566,9 @@ def main():
         return
     if args.mode == "batched-kernel":
         batched_kernel_case(local)
+        return
+    if args.mode == "adjoint-kernel":
+        adjoint_kernel_case(local)
         return
 
     import numpy as np
