@@ -207,8 +207,13 @@ _CHUNK = 1 << 25
 def slater_block(rad, k, la, na, lc, nc, lb, nb, ld, nd, device=None):
     """R^k(a b; c d) for a in states na of la, c in nc of lc (electron 1) and
     b, d likewise (electron 2): [len(na), len(nc), len(nb), len(nd)].  The
-    contraction over the radial grid is one GEMM (on `device` if given); the
-    chi potentials are built in chunks of b."""
+    chi potentials are built from whichever electron has fewer pairs (R^k is
+    symmetric under exchanging the electrons: int rho_ac chi[rho_bd] =
+    int rho_bd chi[rho_ac]); the contraction over the radial grid is one GEMM
+    per pair of the other electron, or one GEMM over chunks of b (on `device`
+    if given)."""
+    if len(na) * len(nc) < len(nb) * len(nd):
+        return _slater_from_electron1(rad, k, la, na, lc, nc, lb, nb, ld, nd, device)
     Pa, Pc = rad.Po[la][na], rad.Po[lc][nc]
     rho1 = (Pa[:, None, :] * Pc[None, :, :] * rad.w).reshape(len(na) * len(nc), -1)
     gm = rad.ri.size
@@ -226,6 +231,28 @@ def slater_block(rad, k, la, na, lc, nc, lb, nb, ld, nd, device=None):
         else:
             R = (rho1_t @ X.reshape(len(bs) * len(nd), -1).T).cpu().numpy()
         out[:, b0:b0 + len(bs), :] = R.reshape(len(na) * len(nc), len(bs), len(nd))
+    return out.reshape(len(na), len(nc), len(nb), len(nd))
+
+
+def _slater_from_electron1(rad, k, la, na, lc, nc, lb, nb, ld, nd, device=None):
+    """R^k(a b; c d) = sum_r w chi[rho_ac](r) P_b(r) P_d(r): the potentials of
+    the (few) electron-1 pairs, then one [nb x q] x [q x nd] GEMM per pair."""
+    X = rad.chi(k, rad.Po[la][na], rad.Po[lc][nc], rad.Pi[la][na], rad.Pi[lc][nc], device)
+    Pb, Pd = rad.Po[lb][nb], rad.Po[ld][nd]
+    nac = len(na) * len(nc)
+    out = np.empty((nac, len(nb), len(nd)))
+    if device is None:
+        wX = X.reshape(nac, -1) * rad.w
+        for i in range(nac):
+            out[i] = (Pb * wX[i]) @ Pd.T
+    else:
+        import torch
+
+        t = lambda a: torch.as_tensor(a, dtype=torch.float64, device=device)  # noqa: E731
+        wX = X.reshape(nac, -1) * t(rad.w)
+        Pb_t, Pd_t = t(Pb), t(Pd)
+        for i in range(nac):
+            out[i] = ((Pb_t * wX[i]) @ Pd_t.T).cpu().numpy()
     return out.reshape(len(na), len(nc), len(nb), len(nd))
 
 
@@ -281,50 +308,50 @@ def v12_matrix(L, idx, rad, k_max="reference", device=None, lmax12=None):
 
 def dipole_2e(Lf, idx_i, idx_f, D1e, gauge):
     """Two-electron dipole block [Ni, Nf] between the configurations of
-    L = Lf - 1 and Lf.  D1e[l]: the d1e block between l and l+1."""
+    L = Lf - 1 and Lf.  D1e[l]: the d1e block between l and l+1.  Built per
+    pair of channels (l1, l2) -> (l1', l2'): the angular conditions are
+    scalars there, and each of the eight terms is a gather of one d1e block
+    masked by the spectator electron's state."""
     Li = Lf - 1
     down = -1.0 if gauge == "v" else 1.0
-    nl = len(D1e)
-    nmax = max(max(d.shape) for d in D1e) if nl else 1
-    D = np.zeros((max(nl, 1), nmax, nmax))
-    for l, d in enumerate(D1e):
-        D[l, :d.shape[0], :d.shape[1]] = d
-    lm = int(max(idx_i[:, [1, 3]].max(), idx_f[:, [1, 3]].max())) + 2
-    six = np.zeros((lm, lm, lm))
-    for la in range(lm):
-        for lb in range(lm):
-            for lf in range(lm):
-                six[la, lb, lf] = wigner_6j(la, lb, Li, Lf, 1, lf)
-    I = {k: idx_i[:, j][:, None] for j, k in enumerate(("n1", "l1", "n2", "l2"))}
-    F = {k: idx_f[:, j][None, :] for j, k in enumerate(("n1", "l1", "n2", "l2"))}
     T = np.zeros((len(idx_i), len(idx_f)))
 
-    def term(la, na, lb, nb, lf, nf, lo, no, ph, up):
-        """One of the eight transition terms: the electron in (na, la) moves
-        to (nf, lf), the other (nb, lb) = (no, lo) is a spectator."""
-        if up:
-            m = (la + 1 == lf) & (lb == lo) & (nb == no)
-            lfix = np.where(m, lf, 1)
-            lq = np.where(m, la, 0)
-            d = D[lq, np.where(m, na, 0), np.where(m, nf, 0)]
-            amp = np.sqrt(4.0 * lfix * lfix - 1.0) / np.sqrt(lfix)
-        else:
-            m = (la - 1 == lf) & (lb == lo) & (nb == no)
-            lfix = np.where(m, la, 1)
-            lq = np.where(m, lf, 0)
-            d = down * D[lq, np.where(m, nf, 0), np.where(m, na, 0)]
-            amp = np.sqrt(4.0 * lfix * lfix - 1.0) / np.sqrt(lfix)
-        s6 = six[np.where(m, la, 0), np.where(m, lb, 0), np.where(m, lf, 0)]
-        sg = np.where(ph % 2 == 1, -1.0, 1.0)
-        return np.where(m, sg * amp * s6 * d, 0.0)
+    def chans(idx):
+        out = {}
+        for q, (n1, l1, n2, l2) in enumerate(idx):
+            out.setdefault((int(l1), int(l2)), []).append(q)
+        return {k: np.array(v) for k, v in out.items()}
 
-    for up in (True, False):
-        phs = ((I["l2"] + F["l1"], I["l1"] + F["l2"], I["l2"] + F["l2"], I["l1"] + F["l1"])
-               if up else (I["l2"] + I["l1"],) * 4)
-        T += term(I["l1"], I["n1"], I["l2"], I["n2"], F["l1"], F["n1"], F["l2"], F["n2"], phs[0], up)
-        T += term(I["l2"], I["n2"], I["l1"], I["n1"], F["l2"], F["n2"], F["l1"], F["n1"], phs[1], up)
-        T += term(I["l1"], I["n1"], I["l2"], I["n2"], F["l2"], F["n2"], F["l1"], F["n1"], phs[2], up)
-        T += term(I["l2"], I["n2"], I["l1"], I["n1"], F["l1"], F["n1"], F["l2"], F["n2"], phs[3], up)
+    ci, cf = chans(idx_i), chans(idx_f)
+    for (l1i, l2i), I in ci.items():
+        n1i, n2i = idx_i[I, 0], idx_i[I, 2]
+        for (l1f, l2f), J in cf.items():
+            n1f, n2f = idx_f[J, 0], idx_f[J, 2]
+            blk = np.zeros((len(I), len(J)))
+            # (moving l, its states, spectator l, its states, final l, final
+            #  states, final spectator l, its states, phase exponent)
+            for up, terms in ((True, ((l1i, n1i, l2i, n2i, l1f, n1f, l2f, n2f, l2i + l1f),
+                                      (l2i, n2i, l1i, n1i, l2f, n2f, l1f, n1f, l1i + l2f),
+                                      (l1i, n1i, l2i, n2i, l2f, n2f, l1f, n1f, l2i + l2f),
+                                      (l2i, n2i, l1i, n1i, l1f, n1f, l2f, n2f, l1i + l1f))),
+                              (False, ((l1i, n1i, l2i, n2i, l1f, n1f, l2f, n2f, l2i + l1i),
+                                       (l2i, n2i, l1i, n1i, l2f, n2f, l1f, n1f, l1i + l2i),
+                                       (l1i, n1i, l2i, n2i, l2f, n2f, l1f, n1f, l2i + l1i),
+                                       (l2i, n2i, l1i, n1i, l1f, n1f, l2f, n2f, l1i + l2i)))):
+                for la, na, lb, nb, lf, nf, lo, no, ph in terms:
+                    if lb != lo or (la + 1 != lf if up else la - 1 != lf):
+                        continue
+                    lm = lf if up else la           # the larger l of the transition
+                    six = wigner_6j(la, lb, Li, Lf, 1, lf)
+                    if six == 0.0:
+                        continue
+                    amp = (-1.0) ** ph * math.sqrt(4.0 * lm * lm - 1.0) / math.sqrt(lm) * six
+                    if up:
+                        d = D1e[la][na[:, None], nf[None, :]]
+                    else:
+                        d = down * D1e[lf][nf[None, :], na[:, None]]
+                    blk += np.where(nb[:, None] == no[None, :], amp * d, 0.0)
+            T[np.ix_(I, J)] = blk
     eqi = (idx_i[:, 0] == idx_i[:, 2]) & (idx_i[:, 1] == idx_i[:, 3])
     eqf = (idx_f[:, 0] == idx_f[:, 2]) & (idx_f[:, 1] == idx_f[:, 3])
     T *= np.where(eqi, math.sqrt(0.5), 1.0)[:, None] * np.where(eqf, math.sqrt(0.5), 1.0)[None, :]
