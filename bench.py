@@ -1,16 +1,16 @@
 #!/usr/bin/env python
 """Benchmark of the B200 `tdse` propagation (one JSON line on rank 0).
 
-Workload (default): the plain 2e helium CI case -- total L = 0..3, blocks of
-3983/4411/4702/4904 states (18000 complex128 coefficients), 61.8M dense
-real64 dipole elements (495 MB), velocity gauge, sin^2 pulse 390 nm
+Workload (default, heci): the plain 2e helium CI case -- He CI inputs built
+first by the library's restated structure chain (400 B-splines of order 9,
+R = 150 a.u., l <= 4, total L = 0..3, inner electron n <= 3: 22,653
+configurations; the 19,053 CI states below 20 a.u. are propagated, 68.4M
+dense real64 dipole elements = 547 MB), velocity gauge, sin^2 pulse 390 nm
 (3.179 eV), 5e14 W/cm^2, 8 cycles, dt = 0.1 with the reference's semantics
 (field frozen at t+dt per step, renormalisation after every step), started
-from the CI ground state.  The H0 spectrum and dipole blocks are seeded
-synthetic data with that layout; --workload heci runs the same pulse on
-genuine He CI inputs that the library's restated structure chain builds
-first (22,653 configurations, ~19k CI states kept; the build is outside the
-timed region).
+from the CI ground state.  The build (~30 s on a B200) is outside the timed
+region.  --workload he2e runs the same pulse on seeded synthetic CI-like
+inputs (18,000 states, 491 MB of couplings) that need no build.
 
 A step is one pulse advanced by one RKF78 step (13 right-hand sides).
   value    pulse-steps/s with the state resident in HBM (mpc_advance);
@@ -558,7 +558,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="he2e", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="heci", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched (256-pulse) measurement")
