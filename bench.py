@@ -239,8 +239,8 @@ def measure_batched(local, stream_cls, rank=0, world=1, dist=None):
                                "path": "mpc_advance, fixed dt=0.1, same system"},
         "ratio_vs_plain": value / plain,
         "whole_job_tflops": 13.0 * 8.0 * S * attempts / sec / 1e12,
-        "tiles": [{"pulses": a, "tile_cols": b, "stages": c, "us_per_rhs": d}
-                  for a, b, c, d in tiles],
+        "tiles": [{"pulses": a, "tile_cols": b, "stages": c, "k_split": d, "us_per_rhs": e}
+                  for a, b, c, d, e in tiles],
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": dmma, "unit": "TFLOP/s",
                      "frac": achieved / dmma, "kernel": "k_batch_stage",
                      "measured_on": "%d pulses at full width over t in [0, 3] a.u. "
@@ -480,8 +480,8 @@ def measure_he2e_batched(local, stream_cls, window=3.0, adj_T=10.0, K=1024):
                     "attempts": attempts, "seconds": sec,
                     "tflops": 13.0 * 8.0 * S * attempts / sec / 1e12,
                     "frac_of_fp64_peak": 13.0 * 8.0 * S * attempts / sec / 1e12 / dmma,
-                    "tiles": [{"pulses": a, "tile_cols": b, "stages": c, "us_per_rhs": d}
-                              for a, b, c, d in tiles]},
+                    "tiles": [{"pulses": a, "tile_cols": b, "stages": c, "k_split": d,
+                               "us_per_rhs": e} for a, b, c, d, e in tiles]},
         "plain_single_pulse": {"value": plain, "unit": UNIT,
                                "path": "mpc_advance (streamed couplings), fixed dt=0.1"},
         "ratio_vs_plain": batched / plain,

@@ -166,12 +166,13 @@ int mpc_batch_propagate(mpc_ctx *ctx, int B, const mpc_pulse *pulses, const doub
 
 /* Tile autotuner of the batched path (new).  Times each tile variant of the
  * batched right-hand side GEMM (pulse-column tile width x cp.async pipeline
- * depth) on this context's system at widths 1, 2, 4, ... up to B pulses and
+ * depth x k split) on this context's system at widths 1, 2, 4, ... up to B pulses and
  * keeps the fastest per width for the context's later batched calls
  * (mpc_batch_propagate runs it on first use; every variant sums in the same
  * order, so the choice never changes results).  If table is non-null it
- * receives up to cap rows of 4 doubles: pulses, tile width (real columns),
- * pipeline depth, microseconds per right-hand side of the chosen variant.
+ * receives up to cap rows of 5 doubles: pulses, tile width (real columns),
+ * pipeline depth, k split (1: the two coupled blocks of a tile run in two
+ * CTAs), microseconds per right-hand side of the chosen variant.
  * Returns the number of rows (>= 0) or an error code. */
 int mpc_batch_autotune(mpc_ctx *ctx, int B, double *table, int cap);
 

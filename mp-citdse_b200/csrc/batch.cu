@@ -231,6 +231,8 @@ struct mpc_batch_state {
   unsigned long long* err = nullptr;
   double* normpart = nullptr;
   int* map = nullptr;
+  double* ws = nullptr;     // split-variant workspace
+  int* cnt = nullptr;       // split-variant arrival counters (kept at zero)
   void* scratch = nullptr;  // compaction staging for per-column scalars
   ColState c{};
   PulseResults res{};
@@ -273,6 +275,8 @@ int ensure_batch(mpc_ctx* c, int B) {
       (rc = balloc(b, &b->out, nel)) || (rc = balloc(b, &b->Fs, (size_t)kNumStages * ldc)) ||
       (rc = balloc(b, &b->err, ldc)) || (rc = balloc(b, &b->normpart, (size_t)nrt * ldc)) ||
       (rc = balloc(b, &b->map, ldc)) ||
+      (rc = balloc(b, &b->ws, split_ws_doubles(nrt, ldc))) ||
+      (rc = balloc(b, &b->cnt, split_cnt_ints(nrt, ldc))) ||
       (rc = balloc(b, reinterpret_cast<char**>(&b->scratch), sizeof(mpc_pulse) * ldc)) ||
       (rc = balloc(b, &s.pulse, ldc)) || (rc = balloc(b, &s.t, ldc)) ||
       (rc = balloc(b, &s.t_end, ldc)) || (rc = balloc(b, &s.h, ldc)) ||
@@ -285,6 +289,7 @@ int ensure_batch(mpc_ctx* c, int B) {
       (rc = balloc(b, &b->res.t, ldc)) || (rc = balloc(b, &b->res.status, ldc)))
     return rc;
   CK(cudaMemsetAsync(b->X, 0, nel * sizeof(double2), c->stream));
+  CK(cudaMemsetAsync(b->cnt, 0, split_cnt_ints(nrt, ldc) * sizeof(int), c->stream));
   CK(cudaMemsetAsync(b->Y[0], 0, nel * sizeof(double2), c->stream));
   CK(cudaMemsetAsync(b->Y[1], 0, nel * sizeof(double2), c->stream));
   CK(cudaMemsetAsync(b->K, 0, nel * kNumStages * sizeof(double2), c->stream));
@@ -313,6 +318,8 @@ StageArgs stage_args(mpc_ctx* c, int s, int ncol, double rtol, double atol, bool
   a.nrowtiles = b->nrowtiles;
   a.want_k_only = k_only ? 1 : 0;
   a.fs_stride = b->ldc;
+  a.ws = b->ws;
+  a.cnt = b->cnt;
   a.g = c->g;
   return a;
 }
@@ -374,6 +381,7 @@ int autotune(mpc_ctx* c, int max_cols) {
 }  // namespace
 
 int mpc_batch_variant(mpc_ctx* c, int ncol) {
+  if (c->forced_variant >= 0 && c->forced_variant < kNumVariants) return c->forced_variant;
   if (c->batch) {
     const std::vector<int>& t = c->batch->tile;
     const int j = width_bucket(ncol);
@@ -423,10 +431,11 @@ int mpc_batch_autotune(mpc_ctx* c, int B, double* table, int cap) {
   const int rows = (int)b->tile.size();
   for (int j = 0; table && j < rows && j < cap; ++j) {
     const int v = b->tile[j];
-    table[4 * j + 0] = std::min(1 << j, b->ldc);
-    table[4 * j + 1] = kVariants[v].bn;
-    table[4 * j + 2] = kVariants[v].nst;
-    table[4 * j + 3] = b->tile_us[(size_t)j * kNumVariants + v];
+    table[5 * j + 0] = std::min(1 << j, b->ldc);
+    table[5 * j + 1] = kVariants[v].bn;
+    table[5 * j + 2] = kVariants[v].nst;
+    table[5 * j + 3] = kVariants[v].split;
+    table[5 * j + 4] = b->tile_us[(size_t)j * kNumVariants + v];
   }
   return rows;
 }

@@ -159,6 +159,8 @@ struct mpc_badj_state {
   double* dpart = nullptr;   // [nchunk][ldc]
   double* dsum = nullptr;    // [ldc]
   unsigned long long* err = nullptr;  // [ldc] (the forward kernel's error slot, unused)
+  double* ws = nullptr;      // split-variant workspace of the stage GEMM
+  int* cnt = nullptr;
   // allocation sizes
   size_t cap_slab = 0, cap_ckpt = 0, cap_seg = 0, cap_steps = 0;
   std::vector<void*> allocs;
@@ -210,7 +212,9 @@ int ensure_badj(mpc_ctx* c, int B, int steps, int ckpt) {
       (rc = fballoc(a, &a->fpart, (size_t)kNumStages * nrt * ldc)) ||
       (rc = fballoc(a, &a->fbar, (size_t)steps * ldc)) ||
       (rc = fballoc(a, &a->dpart, (size_t)nchunk * ldc)) || (rc = fballoc(a, &a->dsum, ldc)) ||
-      (rc = fballoc(a, &a->err, ldc))) {
+      (rc = fballoc(a, &a->err, ldc)) ||
+      (rc = fballoc(a, &a->ws, split_ws_doubles(nrt, ldc))) ||
+      (rc = fballoc(a, &a->cnt, split_cnt_ints(nrt, ldc)))) {
     badj_release(a);
     return rc;
   }
@@ -223,6 +227,7 @@ int ensure_badj(mpc_ctx* c, int B, int steps, int ckpt) {
   CK(cudaMemsetAsync(a->Zbar, 0, sizeof(double2) * slab, c->stream));
   CK(cudaMemsetAsync(a->KB[0], 0, sizeof(double2) * slab, c->stream));
   CK(cudaMemsetAsync(a->KB[1], 0, sizeof(double2) * slab, c->stream));
+  CK(cudaMemsetAsync(a->cnt, 0, sizeof(int) * split_cnt_ints(nrt, ldc), c->stream));
   a->ldc = ldc;
   a->nrt = nrt;
   a->nchunk = nchunk;
@@ -253,6 +258,8 @@ StageArgs fb_args(mpc_ctx* c, int stage, int step) {
   s.nrowtiles = a->nrt;
   s.want_k_only = 0;
   s.fpart = a->fpart;
+  s.ws = a->ws;
+  s.cnt = a->cnt;
   s.g = c->g;
   return s;
 }

@@ -36,12 +36,11 @@ constexpr int kColAlign = 32;   // pulse columns are allocated in multiples of t
 // The narrowest tile covering the active pulses is used, so that a batch
 // whose pulses have mostly retired does not pay for empty columns.
 template <int BN_> struct Tile;
-// KS: independent accumulator sets rotated by k-step.  Every variant keeps
-// KS = 1 so that all tile shapes sum the coupling in the same order and give
-// bit-identical results: the autotuner's choice never changes the numbers.
-template <> struct Tile<64> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 2, KS = 1; };
-template <> struct Tile<32> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 1, KS = 1; };
-template <> struct Tile<16> { static constexpr int WGM = 4, WGN = 2, WMT = 1, WNT = 1, KS = 1; };
+// Every variant sums the coupling in the same order (see the kernel), so
+// the autotuner's choice never changes the numbers.
+template <> struct Tile<64> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 2; };
+template <> struct Tile<32> { static constexpr int WGM = 2, WGN = 4, WMT = 2, WNT = 1; };
+template <> struct Tile<16> { static constexpr int WGM = 4, WGN = 2, WMT = 1, WNT = 1; };
 template <int BN_> constexpr int b_stage() { return BK * (BN_ + 4); }
 // NST_ cp.async stages: 3 for the wide tile (two CTAs per SM), 6 for the
 // narrow ones (small grids: more loads in flight per CTA instead)
@@ -102,10 +101,56 @@ struct StageArgs {
   const double2* Ys;     // the forward stage input y_s
   const double2* Zbar;   // zbar of the step
   double* fpart;         // [13][nrowtiles][ldc] partials of dJ/dF
+  // split variants: the P and Q halves of a tile run in two CTAs; the second
+  // to finish adds the first one's partial (workspace) and runs the epilogue
+  double* ws;            // [row tiles x column tiles][2][BM x BN]
+  int* cnt;              // [row tiles x column tiles] arrivals (left at zero)
   Geometry g;
 };
 
-template <int BN, int NSTB, int MODE>
+
+// One BK-deep chunk of the tile product from shared memory into acc: the A
+// operand is D_{L-1}^T (IS_P, stored k-major) or sign * D_L (stored m-major).
+template <int BN, bool IS_P>
+__device__ __forceinline__ void chunk_mma(const double* As, const double* Bs, int wm, int wn,
+                                          int gq, int tq, double sign,
+                                          double (&acc)[Tile<BN>::WMT][Tile<BN>::WNT][4]) {
+  constexpr int WMT = Tile<BN>::WMT, WNT = Tile<BN>::WNT;
+  constexpr int LDB = BN + 4;
+#pragma unroll
+  for (int ks = 0; ks < BK / 8; ++ks) {
+    double af[WMT][4], bf[WNT][2];
+#pragma unroll
+    for (int mt = 0; mt < WMT; ++mt) {
+      const int m = wm * (WMT * 16) + mt * 16 + gq;
+      const int k = ks * 8 + tq;
+      if constexpr (IS_P) {
+        af[mt][0] = As[k * LDA_P + m];
+        af[mt][1] = As[k * LDA_P + m + 8];
+        af[mt][2] = As[(k + 4) * LDA_P + m];
+        af[mt][3] = As[(k + 4) * LDA_P + m + 8];
+      } else {
+        af[mt][0] = sign * As[m * LDA_Q + k];
+        af[mt][1] = sign * As[(m + 8) * LDA_Q + k];
+        af[mt][2] = sign * As[m * LDA_Q + k + 4];
+        af[mt][3] = sign * As[(m + 8) * LDA_Q + k + 4];
+      }
+    }
+#pragma unroll
+    for (int nt = 0; nt < WNT; ++nt) {
+      const int n = wn * (WNT * 8) + nt * 8 + gq;
+      const int k = ks * 8 + tq;
+      bf[nt][0] = Bs[k * LDB + n];
+      bf[nt][1] = Bs[(k + 4) * LDB + n];
+    }
+#pragma unroll
+    for (int mt = 0; mt < WMT; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < WNT; ++nt) dmma16x8x8(acc[mt][nt], af[mt], bf[nt]);
+  }
+}
+
+template <int BN, int NSTB, int MODE, int SPLIT>
 __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_constant__ StageArgs a) {
   extern __shared__ __align__(16) double bsm[];
   constexpr int WGM = Tile<BN>::WGM, WMT = Tile<BN>::WMT, WNT = Tile<BN>::WNT;
@@ -120,8 +165,15 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   const int gq = lane >> 2, tq = lane & 3;
   const int wm = warp % WGM, wn = warp / WGM;
 
+  // Block index = (row tile, column tile[, k half]) with the column tile and
+  // k half varying fastest: CTAs that read the same coupling rows run side by
+  // side and share them through L2.
+  const int ncolt = (2 * a.ncol + BN - 1) / BN;
+  const int zk = SPLIT ? (int)(blockIdx.x & 1) : 0;
+  const int tp = SPLIT ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;  // tile pair
+  const int rtile = tp / ncolt;
   // row tile -> state block L and first local row r0
-  int L = 0, rt = blockIdx.x;
+  int L = 0, rt = rtile;
   while (true) {
     const int nt = (g.state_off[L + 1] - g.state_off[L] + BM - 1) / BM;
     if (rt < nt || L + 1 >= g.nstate_blk) break;
@@ -130,7 +182,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   }
   const int nL = g.state_off[L + 1] - g.state_off[L];
   const int r0 = rt * BM;
-  const int c0 = blockIdx.y * BN;           // first real column
+  const int c0 = (tp % ncolt) * BN;         // first real column
   const int ncr = 2 * a.ncol;               // real columns in use
   const int ldr = 2 * a.ldc;                // real row pitch of X / Y
   const bool hasP = L > 0, hasQ = L < g.nblk;
@@ -198,79 +250,87 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
     }
   };
 
-  constexpr int KS = Tile<BN>::KS;
-  double acc_k[KS][WM_TILES][WN_TILES][4];
+  // The coupling's two halves accumulate separately -- P (D_{L-1}^T y_{L-1})
+  // and Q (+-D_L y_{L+1}), chunks in order within each -- and are added once,
+  // P + Q, at the end: the same association whether one CTA does both or two
+  // CTAs split them, so every variant gives the same bits.
+  double accP[WM_TILES][WN_TILES][4], accQ[WM_TILES][WN_TILES][4];
 #pragma unroll
-  for (int q = 0; q < KS; ++q)
+  for (int i = 0; i < WM_TILES; ++i)
+#pragma unroll
+    for (int j = 0; j < WN_TILES; ++j)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) accP[i][j][v] = accQ[i][j][v] = 0.0;
+
+  const int ch0 = (SPLIT && zk == 1) ? nchP : 0;
+  const int ch1 = (SPLIT && zk == 0) ? nchP : nch;
+  const int nmine = ch1 - ch0;
+  for (int p = 0; p < NSTB - 1; ++p) {
+    if (p < nmine) load_chunk(ch0 + p, p);
+    cp_commit();
+  }
+  // this CTA's P chunks come first (local indices [0, nPm)), then its Q chunks
+  const int nPm = (SPLIT && zk == 1) ? 0 : nchP;
+  for (int ci = 0; ci < nmine; ++ci) {
+    cp_wait<NSTB - 2>();
+    __syncthreads();
+    {
+      const int nx = ci + NSTB - 1;
+      if (nx < nmine) load_chunk(ch0 + nx, nx % NSTB);
+      cp_commit();
+    }
+    const double* As = bsm + (ci % NSTB) * (A_STAGE + B_STAGE);
+    const double* Bs = As + A_STAGE;
+    if (ci < nPm)
+      chunk_mma<BN, true>(As, Bs, wm, wn, gq, tq, 1.0, accP);
+    else
+      chunk_mma<BN, false>(As, Bs, wm, wn, gq, tq, qsign, accQ);
+  }
+  cp_wait<0>();
+  if constexpr (SPLIT) {
+    // publish this half, then the tile's second arrival takes over
+    constexpr int NACC = WM_TILES * WN_TILES * 4;
+    constexpr int kWsPerCta = BM * BN;  // one CTA's partial tile
+    static_assert(NACC * BTHREADS == kWsPerCta, "workspace slot");
+    const int z = zk;
+    double* mine = a.ws + ((long long)tp * 2 + z) * kWsPerCta;
 #pragma unroll
     for (int i = 0; i < WM_TILES; ++i)
 #pragma unroll
       for (int j = 0; j < WN_TILES; ++j)
 #pragma unroll
-        for (int v = 0; v < 4; ++v) acc_k[q][i][j][v] = 0.0;
-
-  for (int p = 0; p < NSTB - 1; ++p) {
-    if (p < nch) load_chunk(p, p);
-    cp_commit();
-  }
-  for (int ch = 0; ch < nch; ++ch) {
-    cp_wait<NSTB - 2>();
+        for (int v = 0; v < 4; ++v)
+          mine[((i * WN_TILES + j) * 4 + v) * BTHREADS + tid] = z ? accQ[i][j][v] : accP[i][j][v];
+    __threadfence();
     __syncthreads();
-    {
-      const int nx = ch + NSTB - 1;
-      if (nx < nch) load_chunk(nx, nx % NSTB);
-      cp_commit();
+    __shared__ int s_last;
+    if (tid == 0) {
+      const int old = atomicAdd(a.cnt + tp, 1);
+      s_last = (old == 1);
+      if (s_last) a.cnt[tp] = 0;  // ready for the next launch
     }
-    const int st = ch % NSTB;
-    const double* As = bsm + st * (A_STAGE + B_STAGE);
-    const double* Bs = As + A_STAGE;
-    const bool isP = ch < nchP;
-    const double sg = isP ? 1.0 : qsign;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const double* other = a.ws + ((long long)tp * 2 + (1 - z)) * kWsPerCta;
 #pragma unroll
-    for (int ks = 0; ks < BK / 8; ++ks) {
-      double af[WM_TILES][4], bf[WN_TILES][2];
+    for (int i = 0; i < WM_TILES; ++i)
 #pragma unroll
-      for (int mt = 0; mt < WM_TILES; ++mt) {
-        const int m = wm * (WMT * 16) + mt * 16 + gq;
-        const int k = ks * 8 + tq;
-        if (isP) {
-          af[mt][0] = As[k * LDA_P + m];
-          af[mt][1] = As[k * LDA_P + m + 8];
-          af[mt][2] = As[(k + 4) * LDA_P + m];
-          af[mt][3] = As[(k + 4) * LDA_P + m + 8];
-        } else {
-          af[mt][0] = sg * As[m * LDA_Q + k];
-          af[mt][1] = sg * As[(m + 8) * LDA_Q + k];
-          af[mt][2] = sg * As[m * LDA_Q + k + 4];
-          af[mt][3] = sg * As[(m + 8) * LDA_Q + k + 4];
+      for (int j = 0; j < WN_TILES; ++j)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const double o = __ldcg(other + ((i * WN_TILES + j) * 4 + v) * BTHREADS + tid);
+          if (z) accP[i][j][v] = o;
+          else accQ[i][j][v] = o;
         }
-      }
-#pragma unroll
-      for (int nt = 0; nt < WN_TILES; ++nt) {
-        const int n = wn * (WNT * 8) + nt * 8 + gq;
-        const int k = ks * 8 + tq;
-        bf[nt][0] = Bs[k * LDB + n];
-        bf[nt][1] = Bs[(k + 4) * LDB + n];
-      }
-#pragma unroll
-      for (int mt = 0; mt < WM_TILES; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < WN_TILES; ++nt) dmma16x8x8(acc_k[ks % KS][mt][nt], af[mt], bf[nt]);
-    }
   }
-  cp_wait<0>();
   double acc[WM_TILES][WN_TILES][4];
 #pragma unroll
   for (int i = 0; i < WM_TILES; ++i)
 #pragma unroll
     for (int j = 0; j < WN_TILES; ++j)
 #pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        double t = acc_k[0][i][j][v];
-#pragma unroll
-        for (int q = 1; q < KS; ++q) t += acc_k[q][i][j][v];
-        acc[i][j][v] = t;
-      }
+      for (int v = 0; v < 4; ++v) acc[i][j][v] = accP[i][j][v] + accQ[i][j][v];
 
   if constexpr (MODE == 1) {
     // ---------------- adjoint epilogue ----------------
@@ -359,7 +419,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
         double fs = red_f[0][threadIdx.x];
 #pragma unroll
         for (int m = 1; m < BM / 16; ++m) fs += red_f[m][threadIdx.x];
-        a.fpart[((long long)s * a.nrowtiles + blockIdx.x) * a.ldc + q] = fs;
+        a.fpart[((long long)s * a.nrowtiles + rtile) * a.ldc + q] = fs;
       }
     }
     return;
@@ -473,7 +533,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
           const double e = red_e[w][threadIdx.x];
           em = (em != em) ? em : ((e != e) ? e : fmax(em, e));
         }
-        a.normpart[(long long)blockIdx.x * a.ldc + q] = ns;
+        a.normpart[(long long)rtile * a.ldc + q] = ns;
         atomicMax(&a.err[q], (unsigned long long)__double_as_longlong(em));
       }
     }
@@ -484,9 +544,10 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
 // Stage-GEMM variants: pulse-column tile width (real columns) and cp.async
 // pipeline depth.  Three-stage variants fit two CTAs per SM.
 struct TileVariant {
-  int bn, nst;
+  int bn, nst, split;
 };
-constexpr TileVariant kVariants[] = {{16, 3}, {16, 6}, {32, 3}, {32, 6}, {64, 3}};
+constexpr TileVariant kVariants[] = {{16, 3, 0}, {16, 6, 0}, {32, 3, 0}, {32, 6, 0}, {64, 3, 0},
+                                     {16, 6, 1}, {32, 6, 1}, {32, 3, 1}, {64, 3, 1}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 inline int width_bucket(int ncol) {
@@ -501,37 +562,57 @@ inline int default_variant(int ncol) {
   return ncr <= 16 ? 1 : (ncr <= 128 ? 3 : 4);
 }
 
-template <int BN, int NST, int MODE>
+template <int BN, int NST, int MODE, int SPLIT>
 cudaError_t launch_tile(cudaStream_t st, const StageArgs& a) {
-  const int ncr = 2 * a.ncol;
-  return mpc_launch_pdl(k_batch_stage<BN, NST, MODE>, dim3(a.nrowtiles, (ncr + BN - 1) / BN),
-                        dim3(BTHREADS), batch_smem<BN, NST>(), st, a);
+  const int ncolt = (2 * a.ncol + BN - 1) / BN;
+  return mpc_launch_pdl(k_batch_stage<BN, NST, MODE, SPLIT>,
+                        dim3(a.nrowtiles * ncolt * (SPLIT ? 2 : 1)), dim3(BTHREADS),
+                        batch_smem<BN, NST>(), st, a);
 }
 
 template <int MODE>
 cudaError_t launch_variant(cudaStream_t st, int v, const StageArgs& a) {
   switch (v) {
-    case 0: return launch_tile<16, 3, MODE>(st, a);
-    case 1: return launch_tile<16, 6, MODE>(st, a);
-    case 2: return launch_tile<32, 3, MODE>(st, a);
-    case 3: return launch_tile<32, 6, MODE>(st, a);
-    default: return launch_tile<64, 3, MODE>(st, a);
+    case 0: return launch_tile<16, 3, MODE, 0>(st, a);
+    case 1: return launch_tile<16, 6, MODE, 0>(st, a);
+    case 2: return launch_tile<32, 3, MODE, 0>(st, a);
+    case 3: return launch_tile<32, 6, MODE, 0>(st, a);
+    case 4: return launch_tile<64, 3, MODE, 0>(st, a);
+    case 5: return launch_tile<16, 6, MODE, 1>(st, a);
+    case 6: return launch_tile<32, 6, MODE, 1>(st, a);
+    case 7: return launch_tile<32, 3, MODE, 1>(st, a);
+    default: return launch_tile<64, 3, MODE, 1>(st, a);
   }
+}
+
+// Workspace of the split variants for nrowtiles row tiles and ldc pulse
+// columns: two BM x BN partial tiles per tile pair, at most 2 ldc + 64 real
+// columns of tiles whatever BN is; the finest column tiling (16) sets the
+// number of arrival counters.
+inline size_t split_ws_doubles(int nrowtiles, int ldc) {
+  return (size_t)nrowtiles * (2 * ldc + 64) * 2 * BM;
+}
+inline size_t split_cnt_ints(int nrowtiles, int ldc) {
+  return (size_t)nrowtiles * ((2 * ldc + 15) / 16);
 }
 
 template <int MODE>
 cudaError_t set_stage_attrs() {
   cudaError_t e;
-#define MPC_STAGE_ATTR(BN, NST)                                                          \
-  if ((e = cudaFuncSetAttribute(k_batch_stage<BN, NST, MODE>,                            \
+#define MPC_STAGE_ATTR(BN, NST, SPLIT)                                                   \
+  if ((e = cudaFuncSetAttribute(k_batch_stage<BN, NST, MODE, SPLIT>,                     \
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,             \
                                 batch_smem<BN, NST>())) != cudaSuccess)                  \
     return e;
-  MPC_STAGE_ATTR(16, 3)
-  MPC_STAGE_ATTR(16, 6)
-  MPC_STAGE_ATTR(32, 3)
-  MPC_STAGE_ATTR(32, 6)
-  MPC_STAGE_ATTR(64, 3)
+  MPC_STAGE_ATTR(16, 3, 0)
+  MPC_STAGE_ATTR(16, 6, 0)
+  MPC_STAGE_ATTR(32, 3, 0)
+  MPC_STAGE_ATTR(32, 6, 0)
+  MPC_STAGE_ATTR(64, 3, 0)
+  MPC_STAGE_ATTR(16, 6, 1)
+  MPC_STAGE_ATTR(32, 6, 1)
+  MPC_STAGE_ATTR(32, 3, 1)
+  MPC_STAGE_ATTR(64, 3, 1)
 #undef MPC_STAGE_ATTR
   return cudaSuccess;
 }

@@ -72,6 +72,9 @@ struct mpc_ctx {
   struct mpc_badj_state* badj = nullptr;  // batched objective / adjoint (batch_adjoint.cu)
   int path = 0;  // 0 automatic, 1 streaming, 2 resident (MPC_PATH_*)
   double yield_thr = 0.0;  // yield objective: 1 - sum over states below this energy
+  // MPC_BATCH_VARIANT=v at context creation pins the stage-GEMM tile variant
+  // (tests check that every variant gives the same bits); -1: tuned/default
+  int forced_variant = -1;
 };
 
 // Launch with programmatic stream serialization (see mpc_tdse.cu).

@@ -278,12 +278,12 @@ class Context:
 
     def batch_autotune(self, B):
         """Tunes the batched GEMM tiles up to B pulses; returns rows of
-        (pulses, tile width in real columns, pipeline depth, us per RHS)."""
+        (pulses, tile width in real columns, pipeline depth, k split, us per RHS)."""
         cap = 32
-        tab = np.zeros((cap, 4))
+        tab = np.zeros((cap, 5))
         r = lib().mpc_batch_autotune(self._h, int(B), _ptr(tab), cap)
         _check(min(r, 0))
-        return [(int(a), int(b), int(c), float(d)) for a, b, c, d in tab[:r]]
+        return [(int(a), int(b), int(c), int(d), float(e)) for a, b, c, d, e in tab[:r]]
 
     def batch_propagate(self, pulses, t0, t_end, X, h0=0.05, dt_max=0.2, rtol=1e-10,
                         atol=1e-10, max_attempts=0):

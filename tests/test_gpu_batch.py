@@ -159,8 +159,42 @@ def test_autotune_table_and_variants_bit_identical(monkeypatch):
 
     (Xa, acca, _, _), tab = run([])
     assert [r[0] for r in tab] == [1, 2, 4, 8, 16, 32, 64]
-    assert all(r[1] in (16, 32, 64) and r[2] in (3, 6) and r[3] > 0 for r in tab)
+    assert all(r[1] in (16, 32, 64) and r[2] in (3, 6) and r[3] in (0, 1) and r[4] > 0
+               for r in tab)
     for env in (["MPC_NO_AUTOTUNE"], ["MPC_NO_GRAPH"], ["MPC_NO_AUTOTUNE", "MPC_NO_GRAPH"]):
         (Xb, accb, _, _), _ = run(env)
         assert np.array_equal(acca, accb), env
         assert np.array_equal(Xa, Xb), env
+
+
+def test_every_tile_variant_gives_the_same_bits(monkeypatch):
+    """MPC_BATCH_VARIANT pins one of the nine stage-GEMM variants (column
+    tile 16/32/64 x pipeline depth, with or without the P/Q halves in two
+    CTAs): the batched forward and the batched adjoint must not change by a
+    bit, on a 2e system whose blocks have different sizes and row-tile tails."""
+    from mpc_tdse.systems import helium_like_2e
+
+    s = helium_like_2e((70, 90, 100), gauge="v", seed=4)
+    rng = np.random.default_rng(8)
+    specs = [(10 ** rng.uniform(13.5, 14.5), rng.uniform(1.5, 3.0), 1, rng.uniform(0, 6))
+             for _ in range(11)]
+    ps = _pulses("v", specs)
+    pulses = [p for p, _ in ps]
+    t_end = [min(tau, 8.0) for _, tau in ps]
+    X0 = np.zeros((len(ps), s.ntot), complex)
+    X0[:, 0] = 1.0
+    U = np.stack([rng.standard_normal(24) * 0.01 * p.Eo for p in pulses])
+    T = np.full(len(ps), 6.0)
+    out = []
+    for v in range(9):
+        monkeypatch.setenv("MPC_BATCH_VARIANT", str(v))
+        with mpc_tdse.Context.from_system(s) as ctx:
+            ctx.set_path("streaming")
+            X, acc, rej, _ = ctx.batch_propagate(pulses, 0.0, t_end, X0, h0=0.05, dt_max=0.15,
+                                                 rtol=1e-10, atol=1e-10)
+            J, G, Fb = ctx.batch_objective_gradient(pulses, U, T, 0.0, 0.1, 60, X0, -1,
+                                                    ckpt_every=16)
+        out.append((X, acc, rej, J, G, Fb))
+    for v in range(1, 9):
+        for a, b in zip(out[0], out[v]):
+            assert np.array_equal(a, b), v
