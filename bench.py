@@ -255,11 +255,13 @@ def measure_batched(local, stream_cls, rank=0, world=1, dist=None):
 def batched_kernel_case(local):
     """A short batched run for profilers (no autotuning launches, so the
     launch list is the propagation alone): 256 pulses of the batched workload
-    over t in [0, 1] a.u. (stage GEMM at full width, 64-column tiles), then 4
-    of them over [0, 2] a.u. (the persistent resident kernel)."""
+    over t in [0, 1] a.u. (stage GEMM at full width, pinned to the variant the
+    tuner picks there on a B200: 32-column tiles, 3-deep ring, no k split), then
+    4 of them over [0, 2] a.u. (the persistent resident kernel)."""
     import numpy as np
 
     os.environ["MPC_NO_AUTOTUNE"] = "1"
+    os.environ["MPC_BATCH_VARIANT"] = "2"
     import mpc_tdse
     from mpc_tdse.structure1e import hydrogen
 
