@@ -19,7 +19,7 @@ namespace mpc {
 constexpr int kMaxBlocks = 16;      // angular-momentum blocks L = 0..15
 constexpr int kStripW = 256;        // tile width (columns, doubles)
 constexpr int kTileR = 16;          // tile height (rows)
-constexpr int kStages = 6;          // TMA ring depth
+constexpr int kStages = 4;          // TMA ring depth
 constexpr int kConsumerWarps = 8;   // warps that compute; one more issues TMA
 constexpr int kStreamThreads = (kConsumerWarps + 1) * 32;
 constexpr int kTileBytes = kTileR * kStripW * 8;
