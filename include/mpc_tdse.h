@@ -164,6 +164,20 @@ int mpc_batch_propagate(mpc_ctx *ctx, int B, const mpc_pulse *pulses, const doub
                         int max_attempts, double *ct, int *accepted, int *rejected,
                         double *t_final);
 
+/* Single-pulse adaptive RKF78 (new: the reference steps with a fixed dt):
+ * mpc_batch_propagate with B = 1 and the pulse's own t0, t_end; ct: host
+ * [2*size] in/out; accepted / rejected / t_final (optional) are scalars. */
+int mpc_propagate_adaptive(mpc_ctx *ctx, const mpc_pulse *pulse, double t0, double t_end,
+                           double h0, double dt_max, double rtol, double atol, int max_attempts,
+                           double *ct, int *accepted, int *rejected, double *t_final);
+
+/* The batched adaptive propagation under the name of the propagate family;
+ * arguments and results exactly as mpc_batch_propagate. */
+int mpc_propagate_batch(mpc_ctx *ctx, int B, const mpc_pulse *pulses, const double *t0,
+                        const double *t_end, double h0, double dt_max, double rtol, double atol,
+                        int max_attempts, double *ct, int *accepted, int *rejected,
+                        double *t_final);
+
 /* Tile autotuner of the batched path (new).  Times each tile variant of the
  * batched right-hand side GEMM (pulse-column tile width x cp.async pipeline
  * depth x k split) on this context's system at widths 1, 2, 4, ... up to B pulses and
@@ -203,6 +217,13 @@ int mpc_objective_backward(mpc_ctx *ctx, double *grad_u, double *dJdF);
 int mpc_objective_gradient(mpc_ctx *ctx, const mpc_pulse *pulse, int K, const double *u,
                            double T, double t0, double dt, int steps, int target, int ckpt_every,
                            const double *ct0, double *J, double *grad_u, double *dJdF);
+
+/* One call from controls to gradient: exactly mpc_objective_gradient
+ * (objective J, dJ/du and dJ/dF_n of one pulse by the checkpointed discrete
+ * adjoint). */
+int mpc_adjoint(mpc_ctx *ctx, const mpc_pulse *pulse, int K, const double *u, double T,
+                double t0, double dt, int steps, int target, int ckpt_every, const double *ct0,
+                double *J, double *grad_u, double *dJdF);
 
 /* Batched objective and gradient (new).  B pulses at once with the semantics
  * of mpc_objective / mpc_objective_backward per pulse: pulse b has its own

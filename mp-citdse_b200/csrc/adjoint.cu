@@ -574,4 +574,11 @@ int mpc_objective_gradient(mpc_ctx* c, const mpc_pulse* p, int K, const double* 
   return mpc_objective_backward(c, grad_u, dJdF);
 }
 
+int mpc_adjoint(mpc_ctx* c, const mpc_pulse* p, int K, const double* u, double T, double t0,
+                double dt, int steps, int target, int ckpt_every, const double* ct0, double* J,
+                double* grad_u, double* dJdF) {
+  return mpc_objective_gradient(c, p, K, u, T, t0, dt, steps, target, ckpt_every, ct0, J, grad_u,
+                                dJdF);
+}
+
 }  // extern "C"

@@ -421,6 +421,22 @@ int mpc_batch_rhs(mpc_ctx* c, int B, const double* F, const double* x, double* d
   return MPC_OK;
 }
 
+int mpc_propagate_adaptive(mpc_ctx* c, const mpc_pulse* pulse, double t0, double t_end,
+                           double h0, double dt_max, double rtol, double atol, int max_attempts,
+                           double* ct, int* accepted, int* rejected, double* t_final) {
+  if (!pulse || !ct) return mpc_fail(MPC_ERR_ARG, "bad argument");
+  return mpc_batch_propagate(c, 1, pulse, &t0, &t_end, h0, dt_max, rtol, atol, max_attempts, ct,
+                             accepted, rejected, t_final);
+}
+
+int mpc_propagate_batch(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0,
+                        const double* t_end, double h0, double dt_max, double rtol, double atol,
+                        int max_attempts, double* ct, int* accepted, int* rejected,
+                        double* t_final) {
+  return mpc_batch_propagate(c, B, pulses, t0, t_end, h0, dt_max, rtol, atol, max_attempts, ct,
+                             accepted, rejected, t_final);
+}
+
 int mpc_batch_autotune(mpc_ctx* c, int B, double* table, int cap) {
   if (!c || B <= 0 || (table && cap < 0)) return mpc_fail(MPC_ERR_ARG, "bad argument");
   CK(cudaSetDevice(c->device));

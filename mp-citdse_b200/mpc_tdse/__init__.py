@@ -102,6 +102,10 @@ def lib():
     L.mpc_batch_propagate.argtypes = [C.c_void_p, C.c_int, C.POINTER(Pulse), _dp, _dp, C.c_double,
                                       C.c_double, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
                                       _dp]
+    L.mpc_propagate_batch.argtypes = L.mpc_batch_propagate.argtypes
+    L.mpc_propagate_adaptive.argtypes = [C.c_void_p, C.POINTER(Pulse), C.c_double, C.c_double,
+                                         C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                         _dp, _ip, _ip, _dp]
     L.mpc_probe_fp64_peak.argtypes = [C.c_int, _dp, _dp]
     L.mpc_pes.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp, C.c_int, _dp]
     L.mpc_ctx_set_path.argtypes = [C.c_void_p, C.c_int]
@@ -112,6 +116,7 @@ def lib():
     L.mpc_objective_gradient.argtypes = [C.c_void_p, C.POINTER(Pulse), C.c_int, _dp, C.c_double,
                                          C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp,
                                          _dp, _dp, _dp]
+    L.mpc_adjoint.argtypes = L.mpc_objective_gradient.argtypes
     L.mpc_launch_count.restype = C.c_longlong
     L.mpc_launch_count.argtypes = [C.c_void_p]
     _lib = L
@@ -302,6 +307,17 @@ class Context:
                                          atol, int(max_attempts), _ptr(xf), acc.ctypes.data_as(_ip),
                                          rej.ctypes.data_as(_ip), _ptr(tf)))
         return xf.view(np.complex128).reshape(B, -1), acc, rej, tf
+
+    def propagate_adaptive(self, pulse, t0, t_end, x, h0=0.05, dt_max=0.2, rtol=1e-10,
+                           atol=1e-10, max_attempts=0):
+        """Adaptive RKF78 of one pulse (mpc_propagate_adaptive).  Returns
+        (x_final, accepted, rejected, t_final)."""
+        xf = _state(x).copy()
+        acc, rej, tf = C.c_int(), C.c_int(), C.c_double()
+        _check(lib().mpc_propagate_adaptive(self._h, C.byref(pulse), t0, t_end, h0, dt_max, rtol,
+                                            atol, int(max_attempts), _ptr(xf), C.byref(acc),
+                                            C.byref(rej), C.byref(tf)))
+        return xf.view(np.complex128), acc.value, rej.value, tf.value
 
     # -- photoelectron spectrum ---------------------------------------------
     def pes(self, electrons=1, threshold=0.0, ct=None):

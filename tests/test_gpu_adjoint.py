@@ -148,3 +148,27 @@ def test_resident_and_streamed_adjoints_agree():
     assert abs(J1 - J2) < 1e-14
     assert np.max(np.abs(g1 - g2)) <= 1e-12 * np.max(np.abs(g2))
     assert np.max(np.abs(f1 - f2)) <= 1e-12 * np.max(np.abs(f2))
+
+
+def test_mpc_adjoint_is_the_objective_gradient():
+    """mpc_adjoint (one call from controls to gradient) returns exactly what
+    mpc_objective_gradient returns."""
+    import ctypes as C
+
+    s, p, u, T, x0, steps = _problem("v", seed=3, steps=120)
+    L = mpc_tdse.lib()
+    xs = x0.astype(np.complex128).view(np.float64).copy()
+    out = []
+    with mpc_tdse.Context.from_system(s) as ctx:
+        for fn in (L.mpc_objective_gradient, L.mpc_adjoint):
+            J = np.zeros(1)
+            g = np.zeros(len(u))
+            f = np.zeros(steps)
+            dp = C.POINTER(C.c_double)
+            rc = fn(ctx._h, C.byref(p), len(u), u.ctypes.data_as(dp), T, 0.0, 0.1, steps, -1, 32,
+                    xs.ctypes.data_as(dp), J.ctypes.data_as(dp), g.ctypes.data_as(dp),
+                    f.ctypes.data_as(dp))
+            assert rc == 0, mpc_tdse.last_error()
+            out.append((J, g, f))
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)

@@ -198,3 +198,42 @@ def test_every_tile_variant_gives_the_same_bits(monkeypatch):
     for v in range(1, 9):
         for a, b in zip(out[0], out[v]):
             assert np.array_equal(a, b), v
+
+
+def test_single_pulse_adaptive_and_batch_names():
+    """mpc_propagate_adaptive is the batched path with one pulse, and
+    mpc_propagate_batch is mpc_batch_propagate: the same bits."""
+    import ctypes as C
+
+    s = hydrogen_like_1e(60, 3, gauge="l", seed=5)
+    ps = _pulses("l", [(2e13, 1.8, 1, 0.4), (5e13, 2.4, 1, 1.1)])
+    X0 = np.zeros((2, s.ntot), complex)
+    X0[:, 0] = 1.0
+    t_end = [min(tau, 15.0) for _, tau in ps]
+    with mpc_tdse.Context.from_system(s) as ctx:
+        ctx.set_path("streaming")
+        Xb, accb, rejb, tfb = ctx.batch_propagate([ps[0][0]], 0.0, [t_end[0]], X0[:1], h0=0.05,
+                                                  dt_max=0.2)
+        x1, acc1, rej1, tf1 = ctx.propagate_adaptive(ps[0][0], 0.0, t_end[0], X0[0], h0=0.05,
+                                                     dt_max=0.2)
+        assert np.array_equal(Xb[0], x1) and accb[0] == acc1 and rejb[0] == rej1
+        assert tfb[0] == tf1
+        L = mpc_tdse.lib()
+        arr = (mpc_tdse.Pulse * 2)(*[p for p, _ in ps])
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        t0 = np.zeros(2)
+        te = np.array(t_end)
+        res = []
+        for fn in (L.mpc_batch_propagate, L.mpc_propagate_batch):
+            xf = X0.view(np.float64).copy()
+            acc = np.zeros(2, np.int32)
+            rej = np.zeros(2, np.int32)
+            tf = np.zeros(2)
+            rc = fn(ctx._h, 2, arr, t0.ctypes.data_as(dp), te.ctypes.data_as(dp), 0.05, 0.2,
+                    1e-10, 1e-10, 0, xf.ctypes.data_as(dp), acc.ctypes.data_as(ip),
+                    rej.ctypes.data_as(ip), tf.ctypes.data_as(dp))
+            assert rc == 0, mpc_tdse.last_error()
+            res.append((xf, acc, rej, tf))
+        for a, b in zip(*res):
+            assert np.array_equal(a, b)
