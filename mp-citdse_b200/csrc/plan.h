@@ -25,7 +25,10 @@ constexpr int kStreamThreads = (kConsumerWarps + 1) * 32;
 constexpr int kTileBytes = kTileR * kStripW * 8;
 constexpr int kYRowBytes = kTileR * 16;          // the tile's stage-vector rows
 constexpr int kRedBytes = kConsumerWarps * kStripW * 16;
-constexpr int kStreamSmem = kStages * (kTileBytes + kYRowBytes) + kRedBytes + 2 * kStages * 8;
+constexpr int kRpRows = 512;        // row partials staged per bulk store
+constexpr int kRpStageBytes = 2 * kRpRows * 16;
+constexpr int kStreamSmem =
+    kStages * (kTileBytes + kYRowBytes) + kRedBytes + kRpStageBytes + 2 * kStages * 8;
 constexpr int kVecPad = kTileR;     // zeroed tail of every stage vector (row bulk copies)
 constexpr int kNumStages = 13;      // RKF78 stages
 constexpr int kCombineThreads = 256;

@@ -17,7 +17,9 @@
 // of each tile; lane l holds the 8 columns {64j + 2l, 64j + 2l + 1}, j<4, of
 // the current strip.
 //   - Row partials are complete for the strip after a 6-shuffle
-//     reduce-scatter across the warp and are stored to RP[strip][row].
+//     reduce-scatter across the warp; they are staged in shared memory (two
+//     buffers of kRpRows rows) and written to RP[strip][row] by one bulk
+//     store per run of consecutive rows.
 //   - Column partials accumulate in registers while the CTA walks down a
 //     strip; when the strip (or the CTA's range) ends, the 8 warps' partials
 //     are summed in shared memory (warp order 0..7) and stored as one slot
@@ -44,8 +46,10 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   double* tiles = reinterpret_cast<double*>(smem);
   double2* yrows = reinterpret_cast<double2*>(smem + kStages * kTileBytes);
   double2* red = reinterpret_cast<double2*>(smem + kStages * (kTileBytes + kYRowBytes));
-  uint64_t* full =
-      reinterpret_cast<uint64_t*>(smem + kStages * (kTileBytes + kYRowBytes) + kRedBytes);
+  double2* rpbuf =
+      reinterpret_cast<double2*>(smem + kStages * (kTileBytes + kYRowBytes) + kRedBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * (kTileBytes + kYRowBytes) +
+                                               kRedBytes + kRpStageBytes);
   uint64_t* empty = full + kStages;
 
   const Geometry& g = a.g;
@@ -143,6 +147,28 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
     (void)b;
   };
 
+  // Row partials of the current run of consecutive rows [seg_r0, seg_r0 +
+  // seg_n) of strip seg_s of block seg_b, staged in rpbuf[rp_cur]; flushed by
+  // one bulk store when the run ends or the buffer is full.  The store of
+  // the other buffer must have read its rows before that buffer is reused.
+  int rp_cur = 0, seg_b = -1, seg_s = 0, seg_r0 = 0, seg_n = 0;
+  auto flush_rows = [&]() {
+    if (seg_n == 0) return;
+    fence_proxy_async_smem();
+    named_bar_sync(2, kConsumerWarps * 32);
+    if (ctid == 0) {
+      const BlockGeom& sb = g.blk[seg_b];
+      const int nv = min(seg_n, sb.nrow - seg_r0);  // rows past the block's end are not stored
+      bulk_store(a.RP + sb.rp_off + (long long)seg_s * sb.nrow + seg_r0, rpbuf + rp_cur * kRpRows,
+                 (uint32_t)nv * 16u);
+      bulk_commit();
+      bulk_wait_read<1>();
+    }
+    named_bar_sync(2, kConsumerWarps * 32);
+    rp_cur ^= 1;
+    seg_n = 0;
+  };
+
   // After a timed-out wait the warp keeps walking its tiles without reading
   // shared memory, so that every consumer warp still reaches each named
   // barrier; the raised status makes the host discard the result.
@@ -152,6 +178,14 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
     int b, s, rt;
     decode_tile(g, t, b, s, rt);
     const BlockGeom& bg = g.blk[b];
+    if (b != seg_b || s != seg_s || seg_n == kRpRows || rt * kTileR != seg_r0 + seg_n) {
+      flush_rows();
+      seg_b = b;
+      seg_s = s;
+      seg_r0 = rt * kTileR;
+    }
+    const int rp_local = rt * kTileR - seg_r0;  // this tile's first row in the buffer
+    seg_n += kTileR;
     if (b != cur_b || s != cur_s) {
       if (cur_b >= 0) flush_cols(cur_b);
       ++slot;
@@ -167,7 +201,6 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
         }
       }
     }
-    const int r0 = rt * kTileR + 2 * warp;
     const int stage = it % kStages;
     const int round = it / kStages;
     if (!dead && !mbar_wait_bounded(&full[stage], round & 1, a.status)) dead = true;
@@ -211,14 +244,14 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
     z += __shfl_xor_sync(0xffffffffu, z, 2);
     z += __shfl_xor_sync(0xffffffffu, z, 1);
     if ((lane & 7) == 0) {
-      const int r = r0 + (hi16 ? 1 : 0);
-      if (r < bg.nrow) {
-        double* rp = reinterpret_cast<double*>(a.RP + bg.rp_off + (long long)s * bg.nrow + r);
-        rp[hi8 ? 1 : 0] = z;
-      }
+      double* rp = reinterpret_cast<double*>(rpbuf + rp_cur * kRpRows + rp_local + 2 * warp +
+                                             (hi16 ? 1 : 0));
+      rp[hi8 ? 1 : 0] = z;
     }
   }
   if (cur_b >= 0) flush_cols(cur_b);
+  flush_rows();
+  if (ctid == 0) bulk_wait<0>();  // the last stores complete before the grid does
 }
 
 }  // namespace mpc
