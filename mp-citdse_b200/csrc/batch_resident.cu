@@ -82,19 +82,7 @@ __device__ bool br_sync(const BrArgs& a, unsigned long long& epoch, int* s_dead)
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned long long* ctr = reinterpret_cast<unsigned long long*>(a.bar);
-    const unsigned long long target = (epoch + 1) * gridDim.x;
-    asm volatile("fence.acq_rel.gpu;" ::: "memory");  // this CTA's writes before the arrival
-    atomicAdd(ctr, 1ull);
-    const unsigned long long t0 = globaltimer_ns();
-    unsigned it = 0;
-    while (*(volatile unsigned long long*)ctr < target) {
-      if ((++it & 1023u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) {
-        atomicOr(a.status, ST_WAIT_TIMEOUT);
-        *s_dead = 1;
-        break;
-      }
-    }
-    asm volatile("fence.acq_rel.gpu;" ::: "memory");  // others' writes after the wait
+    if (!grid_arrive_wait(ctr, (epoch + 1) * gridDim.x, a.status)) *s_dead = 1;
     epoch += 1;
   }
   __syncthreads();

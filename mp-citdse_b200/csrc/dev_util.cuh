@@ -158,6 +158,33 @@ __device__ __forceinline__ void bulk_wait() {
   asm volatile("cp.async.bulk.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// Grid-barrier arrival and wait for thread 0 of a CTA: the e-th barrier of a
+// launch waits until the monotonic 64-bit counter (cleared before the launch)
+// reaches target = e x gridDim.x.  The acquire-release add publishes this
+// CTA's writes (ordered before it by the CTA's own barrier) and, for the last
+// arrival, already sees every other CTA's; the others poll with acquire
+// loads.  Returns false (and raises ST_WAIT_TIMEOUT) if the wait passed
+// kWaitLimitNs.
+__device__ __forceinline__ bool grid_arrive_wait(unsigned long long* ctr, unsigned long long target,
+                                                 unsigned* status) {
+  unsigned long long old;
+  asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;"
+               : "=l"(old)
+               : "l"(ctr), "l"(1ull)
+               : "memory");
+  if (old + 1 >= target) return true;
+  const unsigned long long t0 = globaltimer_ns();
+  for (unsigned it = 0;; ++it) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(ctr) : "memory");
+    if (v >= target) return true;
+    if ((it & 1023u) == 1023u && globaltimer_ns() - t0 > kWaitLimitNs) {
+      atomicOr(status, ST_WAIT_TIMEOUT);
+      return false;
+    }
+  }
+}
+
 // Named barrier among `nthreads` threads (ids 1..15; 0 is __syncthreads).
 __device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");

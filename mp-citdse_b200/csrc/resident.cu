@@ -72,29 +72,12 @@ struct ResArgs {
 // e * gridDim.x, so the last arrival releases everyone with its one atomic
 // (no reset, no second word).  Bounded wait; returns false (status raised) if
 // it timed out.
-__device__ __forceinline__ void fence_acq_rel_gpu() {
-  asm volatile("fence.acq_rel.gpu;" ::: "memory");
-}
-
 __device__ bool bar_sync(unsigned* bar, unsigned* status, unsigned long long& epoch, bool& dead) {
   __syncthreads();
   __shared__ int timed_out;
   if (threadIdx.x == 0) {
-    timed_out = 0;
     unsigned long long* ctr = reinterpret_cast<unsigned long long*>(bar);
-    const unsigned long long target = (epoch + 1) * gridDim.x;
-    fence_acq_rel_gpu();  // this CTA's writes before the arrival
-    atomicAdd(ctr, 1ull);
-    const unsigned long long t0 = globaltimer_ns();
-    unsigned it = 0;
-    while (*(volatile unsigned long long*)ctr < target) {
-      if ((++it & 1023u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) {
-        atomicOr(status, ST_WAIT_TIMEOUT);
-        timed_out = 1;
-        break;
-      }
-    }
-    fence_acq_rel_gpu();  // the other CTAs' writes after the wait
+    timed_out = grid_arrive_wait(ctr, (epoch + 1) * gridDim.x, status) ? 0 : 1;
     epoch += 1;
   }
   __syncthreads();
