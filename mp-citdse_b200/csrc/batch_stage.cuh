@@ -541,8 +541,11 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
 }
 
 
-// Stage-GEMM variants: pulse-column tile width (real columns) and cp.async
-// pipeline depth.  Three-stage variants fit two CTAs per SM.
+// Stage-GEMM variants: pulse-column tile width (real columns), cp.async
+// pipeline depth, and whether the P and Q halves of a tile run in two CTAs
+// (split; the second to finish adds the first one's partial).  Variant v is
+// index v here (MPC_BATCH_VARIANT pins one).  Three-stage variants fit two
+// CTAs per SM.
 struct TileVariant {
   int bn, nst, split;
 };
