@@ -159,3 +159,35 @@ def test_control_perturbation_interpolates_samples(oracle):
     for k in range(33):
         assert abs(oracle.control_eval(u, T, k * g) - u[k]) < 1e-12
     assert oracle.control_eval(u, T, -0.1) == 0.0 and oracle.control_eval(u, T, T + 0.1) == 0.0
+
+
+@pytest.mark.parametrize("g", ["l", "v"])
+@pytest.mark.parametrize("target", [-1, 3])
+def test_oracle_adjoint_matches_its_own_central_differences(oracle, g, target):
+    """The checker's discrete adjoint against central differences of the
+    checker's own forward (h = 1e-6), on the CPU: the GPU adjoint is compared
+    with this gradient, so it is pinned independently here (1e-6 relative)."""
+    s = hydrogen_like_1e(12, 2, gauge=g, seed=4)
+    ev, wc = oracle.units()
+    w = 1.5498 * ev
+    tau = oracle.period(w, 1)
+    kind = "sineEE" if g == "l" else "sineAA"
+    p = oracle.pulse_setup("sine", g, 2e14 * wc, w, 0.0, 1, tau)
+    rng = np.random.default_rng(7)
+    K, steps, dt = 16, 120, 0.1
+    u = rng.standard_normal(K) * 0.01 * p[0]
+    T = steps * dt
+    x0 = np.zeros(s.ntot, complex)
+    x0[0] = 1.0
+    J, grad, _, _ = oracle.objective_gradient(s.n, s.eig, s.dip, g, kind, p, u, T, 0.0, dt,
+                                              steps, x0, target)
+    assert J == oracle.objective(s.n, s.eig, s.dip, g, kind, p, u, T, 0.0, dt, steps, x0, target)
+    h = 1e-6
+    for k in (1, 7, 12):
+        up, um = u.copy(), u.copy()
+        up[k] += h
+        um[k] -= h
+        fd = (oracle.objective(s.n, s.eig, s.dip, g, kind, p, up, T, 0.0, dt, steps, x0, target) -
+              oracle.objective(s.n, s.eig, s.dip, g, kind, p, um, T, 0.0, dt, steps, x0, target)) \
+            / (2 * h)
+        assert abs(fd - grad[k]) <= 1e-6 * np.max(np.abs(grad)), (k, fd, grad[k])
