@@ -31,3 +31,17 @@ def test_truncated_system_and_files(tmp_path):
     np.testing.assert_allclose(e1, s.eig[30:59], atol=1e-12)
     d = io.h5_read(tmp_path / "dat" / "h12v.h5", "d_if", 29, 28)
     np.testing.assert_allclose(d, s.block(1), atol=1e-12)
+
+
+def test_thomas_reiche_kuhn_sum_rule():
+    """Sum over every p state of the basis of the 1s oscillator strengths is 1
+    (one electron), in the length form 2 dE |<p|z|1s>|^2, the velocity form
+    2 |<p|d/dz|1s>|^2 / dE and the mixed form 2 <p|z|1s><p|d/dz|1s>: z|1s> lies
+    in the basis span, so the finite basis keeps the sum rule."""
+    t, Es, Cs = solve_1e(n=60, k=9, R=40.0, Z=1.0, l_max=1)
+    Dl = dipoles_1e(t, 9, Cs, 40.0, "l")[0][0, :]
+    Dv = dipoles_1e(t, 9, Cs, 40.0, "v")[0][0, :]
+    dE = Es[1] - Es[0][0]
+    assert abs((2 * dE * Dl ** 2).sum() - 1.0) < 1e-10
+    assert abs((2 * Dv ** 2 / dE).sum() - 1.0) < 1e-10
+    assert abs((2 * Dl * Dv).sum() - 1.0) < 1e-10
