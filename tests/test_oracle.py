@@ -191,3 +191,42 @@ def test_oracle_adjoint_matches_its_own_central_differences(oracle, g, target):
               oracle.objective(s.n, s.eig, s.dip, g, kind, p, um, T, 0.0, dt, steps, x0, target)) \
             / (2 * h)
         assert abs(fd - grad[k]) <= 1e-6 * np.max(np.abs(grad)), (k, fd, grad[k])
+
+
+def test_pes_restatement_known_answers():
+    """The restated pes binning on hand-made spectra: a 1e state falls in the
+    first l = 1 bin whose half-widths bracket it and adds |c|^2 * 2/(width);
+    a 2e state above the threshold gives its own density |c|^2 * 2/(E+ - E-);
+    the ground population, norm, yield and excited population follow."""
+    from oracle import pes_reference
+
+    # 1e: blocks l = 0, 1, 2 of 6, 6, 3 states; the l = 1 energies form the
+    # grid, whose slots run over 1 <= k <= state_sz[0] - 2 as in the reference
+    E0 = [-0.5, -0.125, 0.05, 0.3, 0.6, 0.8]
+    E1 = [-0.25, -0.1, 0.1, 0.3, 0.5, 0.7]
+    E2 = [-0.05, 0.31, 0.9]
+    eig = np.array(E0 + E1 + E2)
+    ct = np.zeros(15, complex)
+    ct[0] = 0.5                   # ground state (never binned: loops start at 1)
+    ct[3] = 0.4                   # l = 0, E = 0.3: bin k = 3 (E1[3], half-widths 0.1)
+    ct[6 + 2] = 0.3j              # l = 1, E = 0.1: bin k = 2
+    ct[12 + 1] = 0.2              # l = 2, E = 0.31: bin k = 3
+    pes, ground, norm, yld, _ = pes_reference([6, 6, 3], eig, ct, electrons=1)
+    assert ground == 0.25
+    assert abs(norm - (0.25 + 0.16 + 0.09 + 0.04)) < 1e-15
+    assert abs(pes[0, 3] - 0.16 * 2 / 0.4) < 1e-14
+    assert abs(pes[1, 2] - 0.09 * 2 / 0.4) < 1e-14
+    assert abs(pes[2, 3] - 0.04 * 2 / 0.4) < 1e-14
+    assert np.count_nonzero(pes) == 3
+    assert abs(yld - (0.16 + 0.09 + 0.04)) < 1e-15
+    # 2e: one block, threshold -2; states 1..n-2 above it are densities
+    eig2 = np.array([-2.9, -2.1, -1.9, -1.5, -1.0, -0.2])
+    c2 = np.array([0.8, 0.1, 0.2, 0.3, 0.1, 0.5], dtype=complex)
+    pes2, g2, n2, y2, exc2 = pes_reference([6], eig2, c2, electrons=2, threshold=-2.0)
+    assert abs(g2 - 0.64) < 1e-15
+    assert pes2[0, 1] == 0.0                                 # -2.1 is below the threshold
+    assert abs(pes2[0, 2] - 0.04 * 2 / (-1.5 + 2.1)) < 1e-14
+    assert abs(pes2[0, 4] - 0.01 * 2 / (-0.2 + 1.5)) < 1e-14
+    assert pes2[0, 5] == 0.0                                 # the top state has no upper edge
+    assert abs(y2 - (0.04 + 0.09 + 0.01)) < 1e-15
+    assert abs(exc2 - (0.01 + 0.04 + 0.09 + 0.01)) < 1e-15
