@@ -97,6 +97,21 @@ int mpc_ctx_destroy(mpc_ctx *ctx);
 int mpc_ctx_set_path(mpc_ctx *ctx, int path);
 int mpc_ctx_get_path(mpc_ctx *ctx);   /* the path mpc_advance will take */
 
+/* Failure detection (new: the reference has no device code to watch).  The
+ * persistent cooperative kernels (the resident single-pulse propagation, its
+ * adjoint sweep and the resident batched tail) meet at grid barriers whose
+ * waits are bounded: a CTA that waits longer than this limit (default 2 s)
+ * stops, every other CTA stops at its own bounded wait, the call returns
+ * MPC_ERR_DEVICE ("wait timeout") and the context stays usable.  seconds in
+ * [1e-6, 60].  The streaming kernel's TMA ring waits keep a fixed 2 s bound. */
+int mpc_ctx_set_wait_limit(mpc_ctx *ctx, double seconds);
+
+/* Fault injection for tests of the failure detection above: the next
+ * persistent launch on this context gets grid-barrier targets one arrival
+ * beyond what its CTAs can make, so its first barrier wait runs out after the
+ * wait limit and the call reports the timeout.  Later launches are normal. */
+int mpc_ctx_inject_barrier_timeout(mpc_ctx *ctx);
+
 /* Total number of states sum(state_sz). */
 int mpc_ctx_size(const mpc_ctx *ctx);
 
@@ -122,8 +137,10 @@ int mpc_rk78_step(mpc_ctx *ctx, double F, double dt, double *x);
  *                      (the reference's _pop<n><l>.dat column);
  *   field_out[steps]   the field used by each step (_field.dat column);
  *   norm_out[steps]    ||ct|| before each renormalisation (norm drift).
- * Returns MPC_ERR_UNSTABLE if dt*(max|E| + max|F|*||D||) lies outside the
- * RKF78 imaginary-axis stability interval. */
+ * Returns MPC_ERR_UNSTABLE if dt*max|E| lies outside the RKF78
+ * imaginary-axis stability interval (the field coupling widens the spectrum
+ * further; keeping dt inside the interval for H0 + F*D is the caller's job,
+ * as it is in the reference, whose states_in_l truncation serves it). */
 int mpc_propagate(mpc_ctx *ctx, const mpc_pulse *pulse, double t0, double dt, int steps,
                   int pop_index, double *ct, double *pop_out, double *field_out,
                   double *norm_out);
@@ -297,7 +314,10 @@ long long mpc_launch_count(const mpc_ctx *ctx);
  * CUDA device: d_eig [sum(state_sz)], d_dip (blocks back to back, block L
  * row-major [state_sz[L] x state_sz[L+1]]), d_x and d_dxdt [2*sum(state_sz)]
  * doubles.  state_sz is a host array.  Runs asynchronously on `stream`
- * (a cudaStream_t; NULL = the legacy default stream).
+ * (a cudaStream_t; NULL = the legacy default stream).  d_x and d_dxdt must be
+ * 16-byte aligned (they are read and written as complex pairs) and d_eig and
+ * d_dip 8-byte aligned; a misaligned view (say, a slice starting one double
+ * in) is refused with MPC_ERR_ARG before anything is launched.
  *
  * Its scratch is a static device array of MPC_NOALLOC_SCRATCH_BYTES (16 MiB)
  * that every GPU loading the library holds until the process exits.  Systems
@@ -305,7 +325,9 @@ long long mpc_launch_count(const mpc_ctx *ctx);
  * + 256 per column-partial slot) -- or more than 256 column strips are
  * rejected with MPC_ERR_ARG.  The first call on each device looks up the
  * array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture begins.  All calls share the array and it keeps the
+ * any stream capture begins.  The address is cached per CUDA context: after
+ * cudaDeviceReset, or with another context current, the next call looks it up
+ * again (so that call, too, should come before any capture).  All calls share the array and it keeps the
  * last call's contents: calls whose kernels overlap on the GPU race, so
  * serialise them.  No cudaMalloc, cudaFree or host heap allocation. */
 #define MPC_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)

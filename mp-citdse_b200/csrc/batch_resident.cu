@@ -72,6 +72,7 @@ struct BrArgs {
   int ldc, ncol, ntot;
   int exit_below, max_attempts, gauge;
   double rtol, atol, dt_max;
+  BarrierCfg bc;
   Geometry g;
 };
 
@@ -82,7 +83,8 @@ __device__ bool br_sync(const BrArgs& a, unsigned long long& epoch, int* s_dead)
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned long long* ctr = reinterpret_cast<unsigned long long*>(a.bar);
-    if (!grid_arrive_wait(ctr, (epoch + 1) * gridDim.x, a.status)) *s_dead = 1;
+    if (!grid_arrive_wait(ctr, (epoch + 1) * gridDim.x + a.bc.skew, a.status, a.bc.wait_ns))
+      *s_dead = 1;
     epoch += 1;
   }
   __syncthreads();
@@ -639,6 +641,7 @@ int mpc_batch_res_run(mpc_ctx* c, const BatchResLaunch& l, int P, int exit_below
   a.rtol = l.rtol;
   a.atol = l.atol;
   a.dt_max = l.dt_max;
+  a.bc = mpc_barrier_cfg(c);
   a.g = c->g;
   CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned) * 2, c->stream));  // arrival counter
   void* args[] = {&a};

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/mpc_tdse.h"
+#include "dev_util.cuh"
 #include "plan.h"
 #include "stream_types.h"
 
@@ -75,7 +76,16 @@ struct mpc_ctx {
   // MPC_BATCH_VARIANT=v at context creation pins the stage-GEMM tile variant
   // (tests check that every variant gives the same bits); -1: tuned/default
   int forced_variant = -1;
+  // grid-barrier wait limit of the persistent kernels (mpc_ctx_set_wait_limit)
+  unsigned long long wait_limit_ns = 2000000000ull;
+  // the next persistent launch gets an unreachable barrier target
+  // (mpc_ctx_inject_barrier_timeout); cleared when that launch is set up
+  bool inject_barrier_timeout = false;
 };
+
+// Barrier settings for the next persistent launch on c (consumes a pending
+// injected barrier timeout).
+mpc::BarrierCfg mpc_barrier_cfg(mpc_ctx* c);
 
 // Launch with programmatic stream serialization (see mpc_tdse.cu).
 bool mpc_pdl_enabled();

@@ -14,7 +14,9 @@ enum : unsigned {
   ST_BAD_LAUNCH = 4u,     // a kernel saw an inconsistent launch shape
 };
 
-// Upper bound on any single wait, in nanoseconds of %globaltimer.
+// Upper bound on a TMA ring (mbarrier) wait, in nanoseconds of %globaltimer,
+// and the default bound on a grid-barrier wait (the persistent kernels take
+// theirs from the launch arguments: a per-context setting).
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -164,9 +166,10 @@ __device__ __forceinline__ void bulk_wait() {
 // CTA's writes (ordered before it by the CTA's own barrier) and, for the last
 // arrival, already sees every other CTA's; the others poll with acquire
 // loads.  Returns false (and raises ST_WAIT_TIMEOUT) if the wait passed
-// kWaitLimitNs.
+// limit_ns.
 __device__ __forceinline__ bool grid_arrive_wait(unsigned long long* ctr, unsigned long long target,
-                                                 unsigned* status) {
+                                                 unsigned* status,
+                                                 unsigned long long limit_ns = kWaitLimitNs) {
   unsigned long long old;
   asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;"
                : "=l"(old)
@@ -178,12 +181,20 @@ __device__ __forceinline__ bool grid_arrive_wait(unsigned long long* ctr, unsign
     unsigned long long v;
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(ctr) : "memory");
     if (v >= target) return true;
-    if ((it & 1023u) == 1023u && globaltimer_ns() - t0 > kWaitLimitNs) {
+    if ((it & 1023u) == 1023u && globaltimer_ns() - t0 > limit_ns) {
       atomicOr(status, ST_WAIT_TIMEOUT);
       return false;
     }
   }
 }
+
+// The grid-barrier settings of one persistent launch: the wait limit and an
+// extra arrival count added to every target (0; 1 only when a test injects a
+// barrier that cannot complete, so that the bounded wait runs out).
+struct BarrierCfg {
+  unsigned long long wait_ns;
+  unsigned long long skew;
+};
 
 // Named barrier among `nthreads` threads (ids 1..15; 0 is __syncthreads).
 __device__ __forceinline__ void named_bar_sync(int id, int nthreads) {

@@ -410,6 +410,15 @@ int mpc_fill_field_table(mpc_ctx* c, const double* F, int steps) {
 
 bool mpc_use_resident(mpc_ctx* c) { return use_resident(c); }
 
+mpc::BarrierCfg mpc_barrier_cfg(mpc_ctx* c) {
+  mpc::BarrierCfg b{c->wait_limit_ns, 0ull};
+  if (c->inject_barrier_timeout) {
+    b.skew = 1;  // one arrival more than the grid can make: no barrier completes
+    c->inject_barrier_timeout = false;
+  }
+  return b;
+}
+
 extern "C" {
 
 int mpc_version(void) { return 100; }
@@ -586,6 +595,19 @@ int mpc_ctx_destroy(mpc_ctx* c) {
 }
 
 int mpc_ctx_size(const mpc_ctx* c) { return c ? c->g.ntot : MPC_ERR_ARG; }
+
+int mpc_ctx_set_wait_limit(mpc_ctx* c, double seconds) {
+  if (!c || !(seconds >= 1e-6) || !(seconds <= 60.0))
+    return fail(MPC_ERR_ARG, "wait limit must be in [1e-6, 60] s");
+  c->wait_limit_ns = (unsigned long long)(seconds * 1e9);
+  return MPC_OK;
+}
+
+int mpc_ctx_inject_barrier_timeout(mpc_ctx* c) {
+  if (!c) return fail(MPC_ERR_ARG, "null argument");
+  c->inject_barrier_timeout = true;
+  return MPC_OK;
+}
 
 int mpc_ctx_set_path(mpc_ctx* c, int path) {
   if (!c || path < 0 || path > 2) return fail(MPC_ERR_ARG, "bad path");

@@ -64,6 +64,7 @@ struct ResArgs {
   double2* ckpt;           // x every ckpt_every steps: slot k holds x after k*ckpt_every
   int ckpt_every;
   long long vpitch;
+  BarrierCfg bc;
   Geometry g;
 };
 
@@ -72,12 +73,14 @@ struct ResArgs {
 // e * gridDim.x, so the last arrival releases everyone with its one atomic
 // (no reset, no second word).  Bounded wait; returns false (status raised) if
 // it timed out.
-__device__ bool bar_sync(unsigned* bar, unsigned* status, unsigned long long& epoch, bool& dead) {
+__device__ bool bar_sync(unsigned* bar, unsigned* status, const BarrierCfg& bc,
+                         unsigned long long& epoch, bool& dead) {
   __syncthreads();
   __shared__ int timed_out;
   if (threadIdx.x == 0) {
     unsigned long long* ctr = reinterpret_cast<unsigned long long*>(bar);
-    timed_out = grid_arrive_wait(ctr, (epoch + 1) * gridDim.x, status) ? 0 : 1;
+    timed_out =
+        grid_arrive_wait(ctr, (epoch + 1) * gridDim.x + bc.skew, status, bc.wait_ns) ? 0 : 1;
     epoch += 1;
   }
   __syncthreads();
@@ -86,7 +89,7 @@ __device__ bool bar_sync(unsigned* bar, unsigned* status, unsigned long long& ep
 }
 
 __device__ bool grid_sync(const ResArgs& a, unsigned long long& epoch, bool& dead) {
-  return bar_sync(a.bar, a.status, epoch, dead);
+  return bar_sync(a.bar, a.status, a.bc, epoch, dead);
 }
 
 __device__ __forceinline__ double2 ld_cg(const double2* p) { return __ldcg(p); }
@@ -358,6 +361,7 @@ struct AdjResArgs {
   int gauge;
   double dt;
   long long vpitch;
+  BarrierCfg bc;
   Geometry g;
 };
 
@@ -412,7 +416,7 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_adj_resident(const __grid_const
       for (int w = 1; w < RWARPS; ++w) t += red[w];
       a.part[c] = t;
     }
-    if (!bar_sync(a.bar, a.status, epoch, dead)) break;
+    if (!bar_sync(a.bar, a.status, a.bc, epoch, dead)) break;
     if (threadIdx.x < 32) {
       double t = 0.0;
       for (int p = threadIdx.x; p < G; p += 32) t += __ldcg(a.part + p);
@@ -431,7 +435,7 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_adj_resident(const __grid_const
         frow[li] = 0.0;
       }
     }
-    if (!bar_sync(a.bar, a.status, epoch, dead)) break;
+    if (!bar_sync(a.bar, a.status, a.bc, epoch, dead)) break;
     double fcta = 0.0;
     for (int s = kNumStages - 1; s >= 0; --s) {
       const double2* kin = a.kb[s & 1];
@@ -488,7 +492,7 @@ __global__ void __launch_bounds__(RTHREADS, 1) k_adj_resident(const __grid_const
           lams[li] = o;
         }
       }
-      if (s > 0 && !bar_sync(a.bar, a.status, epoch, dead)) break;
+      if (s > 0 && !bar_sync(a.bar, a.status, a.bc, epoch, dead)) break;
       __syncthreads();
     }
     if (dead) break;
@@ -653,6 +657,7 @@ int mpc_resident_run(mpc_ctx* c, double dt, int steps, int pop_index) {
   a.gauge = (c->gauge == 'l') ? 0 : 1;
   a.first_is_normalised = 1;
   a.dt = dt;
+  a.bc = mpc_barrier_cfg(c);
   a.g = c->g;
   CK(cudaMemcpyAsync(r->XN, c->d_x, sizeof(double2) * c->g.ntot, cudaMemcpyDeviceToDevice,
                      c->stream));
@@ -696,6 +701,7 @@ int mpc_resident_forward_ex(mpc_ctx* c, const double2* x_in, double2* x_out, con
   a.ckpt = ckpt;
   a.ckpt_every = ckpt_every > 0 ? ckpt_every : 1;
   a.vpitch = vpitch;
+  a.bc = mpc_barrier_cfg(c);
   a.g = c->g;
   CK(cudaMemcpyAsync(r->XN, x_in, sizeof(double2) * c->g.ntot, cudaMemcpyDeviceToDevice,
                      c->stream));
@@ -742,6 +748,7 @@ int mpc_resident_adjoint(mpc_ctx* c, const double* Ftab, double dt, int len,
   a.gauge = (c->gauge == 'l') ? 0 : 1;
   a.dt = dt;
   a.vpitch = vpitch;
+  a.bc = mpc_barrier_cfg(c);
   a.g = c->g;
   CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned) * 2, c->stream));
   void* args[] = {&a};

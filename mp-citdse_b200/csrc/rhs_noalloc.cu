@@ -19,9 +19,15 @@
 //
 // In host code `g_scratch` is only a host-side stand-in for the device array,
 // not a device address: the address is obtained with cudaGetSymbolAddress on
-// the first call on each device (with that device current) and cached.
+// the first call on each device (with that device current) and cached
+// together with the identity of the CUDA context it belongs to.  When the
+// current context of the device changes (after cudaDeviceReset, or when the
+// caller makes another context current), the module is loaded anew in that
+// context and the address is looked up again.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstdio>
 #include <mutex>
 
@@ -199,13 +205,45 @@ __global__ void __launch_bounds__(256) k_rhs_direct_epilogue(const __grid_consta
 
 std::mutex g_setup_mu;
 void* g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
 int g_num_sms[kMaxDevices] = {};
 
-// First call on a device: look up the device address of g_scratch (with that
-// device current) and the SM count; both are cached for later calls.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+// Identity of the calling thread's current CUDA context (0 when none is
+// current yet), through the driver entry points the runtime exposes.
+unsigned long long current_ctx_id() {
+  static CtxGetCurrentFn get_cur = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_cur = reinterpret_cast<CtxGetCurrentFn>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(p);
+    cudaGetLastError();
+    looked = true;
+  }
+  CUcontext cu = nullptr;
+  if (!get_cur || get_cur(&cu) != CUDA_SUCCESS || !cu) return 0;
+  unsigned long long id = 0;
+  if (get_id && get_id(cu, &id) == CUDA_SUCCESS) return id + 1;
+  return (unsigned long long)(uintptr_t)cu;
+}
+
+// Look up the device address of g_scratch (with device `dev` current) and the
+// SM count on the first call in each CUDA context; both are cached until the
+// device's current context changes.
 int device_setup(int dev, void** scratch, int* sms) {
   std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch_addr[dev]) {
+  const unsigned long long ctx = current_ctx_id();
+  if (!g_scratch_addr[dev] || ctx == 0 || ctx != g_scratch_ctx[dev]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
     if (e != cudaSuccess || !p) {
@@ -220,6 +258,8 @@ int device_setup(int dev, void** scratch, int* sms) {
       return mpc_internal_fail(MPC_ERR_CUDA, "cannot read the SM count");
     g_num_sms[dev] = n;
     g_scratch_addr[dev] = p;
+    // the symbol lookup made the device's primary context current if none was
+    g_scratch_ctx[dev] = ctx ? ctx : current_ctx_id();
   }
   *scratch = g_scratch_addr[dev];
   *sms = g_num_sms[dev];
@@ -242,6 +282,15 @@ extern "C" int mpc_rhs_noalloc(int L_max, const int* state_sz, const double* d_e
     return mpc_internal_fail(MPC_ERR_ARG, "mpc_rhs_noalloc: gauge must be 'l' or 'v'");
   for (int L = 0; L <= L_max; ++L)
     if (state_sz[L] <= 0) return mpc_internal_fail(MPC_ERR_ARG, "mpc_rhs_noalloc: state_sz <= 0");
+  // the kernels read and write x / dxdt as 16-byte complex pairs and the
+  // energies / dipoles as doubles: a misaligned view is refused here, before
+  // any launch, instead of faulting on the device
+  if (((uintptr_t)d_x | (uintptr_t)d_dxdt) & 15u)
+    return mpc_internal_fail(MPC_ERR_ARG,
+                             "mpc_rhs_noalloc: d_x and d_dxdt must be 16-byte aligned");
+  if (((uintptr_t)d_eig | (uintptr_t)d_dip) & 7u)
+    return mpc_internal_fail(MPC_ERR_ARG,
+                             "mpc_rhs_noalloc: d_eig and d_dip must be 8-byte aligned");
 
   // geometry on the stack (nothing is allocated, on the host either)
   DirectArgs da;

@@ -119,6 +119,8 @@ def lib():
     L.mpc_adjoint.argtypes = L.mpc_objective_gradient.argtypes
     L.mpc_launch_count.restype = C.c_longlong
     L.mpc_launch_count.argtypes = [C.c_void_p]
+    L.mpc_ctx_set_wait_limit.argtypes = [C.c_void_p, C.c_double]
+    L.mpc_ctx_inject_barrier_timeout.argtypes = [C.c_void_p]
     _lib = L
     return L
 
@@ -404,6 +406,16 @@ class Context:
         if r < 0:
             _check(r)
         return {1: "streaming", 2: "resident"}[r]
+
+    def set_wait_limit(self, seconds):
+        """Bound on the persistent kernels' grid-barrier waits (default 2 s);
+        a wait that runs out makes the call raise MpcError (MPC_ERR_DEVICE)."""
+        _check(lib().mpc_ctx_set_wait_limit(self._h, float(seconds)))
+
+    def inject_barrier_timeout(self):
+        """Test hook: the next persistent launch gets a grid barrier that
+        cannot complete, so its bounded wait runs out."""
+        _check(lib().mpc_ctx_inject_barrier_timeout(self._h))
 
     def profile(self, on=True):
         _check(lib().mpc_profile_enable(self._h, int(bool(on))))

@@ -69,10 +69,48 @@ def test_noalloc_rejects_systems_beyond_its_scratch():
     L = _bind()
     dev = torch.device("cuda", 0)
     buf = torch.zeros(16, dtype=torch.float64, device=dev)
-    # 3 blocks of 40000 states: the row partials alone need far more than 16 MiB
+    # 3 blocks of 40000 states: 2 x 157 column strips, beyond the 256 the
+    # static partial-slot table holds
     n = np.array([40000, 40000, 40000], dtype=np.int32)
     rc = L.mpc_rhs_noalloc(2, n.ctypes.data_as(C.POINTER(C.c_int)), buf.data_ptr(),
                            buf.data_ptr(), b"l", 0.1, buf.data_ptr(), buf.data_ptr(), None)
     assert rc == -1
-    msg = mpc_tdse.last_error()
-    assert "static maximum" in msg or "column strips" in msg
+    assert "column strips" in mpc_tdse.last_error()
+    # 100 strips, but 100 x 40000 row partials of 16 B = 64 MB: beyond the
+    # 16 MiB static array
+    n = np.array([40000, 25600], dtype=np.int32)
+    rc = L.mpc_rhs_noalloc(1, n.ctypes.data_as(C.POINTER(C.c_int)), buf.data_ptr(),
+                           buf.data_ptr(), b"l", 0.1, buf.data_ptr(), buf.data_ptr(), None)
+    assert rc == -1
+    assert "static maximum" in mpc_tdse.last_error()
+
+
+def test_noalloc_refuses_misaligned_views_before_launch():
+    import torch
+
+    L = _bind()
+    s = random_system([40, 50, 30], gauge="l", seed=5, e_max=8.0)
+    dev = torch.device("cuda", 0)
+    d_eig = torch.from_numpy(s.eig.copy()).to(dev)
+    d_dip = torch.from_numpy(s.dip.copy()).to(dev)
+    d_x = torch.zeros(2 * s.ntot + 2, dtype=torch.float64, device=dev)
+    d_out = torch.zeros(2 * s.ntot + 2, dtype=torch.float64, device=dev)
+    n = np.ascontiguousarray(s.n, dtype=np.int32)
+    np_ = n.ctypes.data_as(C.POINTER(C.c_int))
+    # a complex view starting one double in: 8-byte but not 16-byte aligned
+    for xp, op in ((d_x.data_ptr() + 8, d_out.data_ptr()), (d_x.data_ptr(), d_out.data_ptr() + 8)):
+        rc = L.mpc_rhs_noalloc(len(n) - 1, np_, d_eig.data_ptr(), d_dip.data_ptr(), b"l", 0.2,
+                               xp, op, None)
+        assert rc == -1
+        assert "16-byte aligned" in mpc_tdse.last_error()
+    rc = L.mpc_rhs_noalloc(len(n) - 1, np_, d_eig.data_ptr() + 4, d_dip.data_ptr(), b"l", 0.2,
+                           d_x.data_ptr(), d_out.data_ptr(), None)
+    assert rc == -1
+    assert "8-byte aligned" in mpc_tdse.last_error()
+    # nothing was launched: the output buffer is untouched and the device is fine
+    torch.cuda.synchronize()
+    assert float(d_out.abs().sum()) == 0.0
+    rc = L.mpc_rhs_noalloc(len(n) - 1, np_, d_eig.data_ptr(), d_dip.data_ptr(), b"l", 0.2,
+                           d_x.data_ptr(), d_out.data_ptr(), None)
+    assert rc == 0, mpc_tdse.last_error()
+    torch.cuda.synchronize()
