@@ -181,6 +181,26 @@ int mpc_batch_propagate(mpc_ctx *ctx, int B, const mpc_pulse *pulses, const doub
                         int max_attempts, double *ct, int *accepted, int *rejected,
                         double *t_final);
 
+/* Batched fixed-step propagation with the reference's semantics (new: the
+ * reference runs one pulse per process).  B pulses advance together, each
+ * exactly as mpc_propagate -- the loop of tdse::propV / propL,
+ * src/tdse/tdse.cpp:186-215 -- would advance it alone: per step the field
+ * F_b(t_b + dt) is frozen for the 13 stages, one RKF78 step (8th-order
+ * solution), t_b += dt, c_b /= ||c_b||.  Pulse b runs steps[b] steps from
+ * t0[b]; a pulse that has finished retires and the batch narrows (each stage
+ * is one FP64 tensor-core GEMM over the active pulses; the last few pulses
+ * finish in the persistent resident kernel when the coupling fits on chip).
+ * ct: host [B][2*size] in/out.  Optional host outputs (NULL to skip), with
+ * M = max(steps):
+ *   pop_out [B][M+1]   |c_b[pop_index]|^2 at t0[b] and after every step
+ *                      (the _pop column; entries past steps[b] are unset);
+ *   norm_out [B][M]    ||c_b|| before each renormalisation.
+ * Returns MPC_ERR_DEVICE (non-finite norm) if a pulse's norm stops being
+ * finite, MPC_ERR_UNSTABLE as mpc_propagate does. */
+int mpc_batch_advance(mpc_ctx *ctx, int B, const mpc_pulse *pulses, const double *t0, double dt,
+                      const int *steps, int pop_index, double *ct, double *pop_out,
+                      double *norm_out);
+
 /* Single-pulse adaptive RKF78 (new: the reference steps with a fixed dt):
  * mpc_batch_propagate with B = 1 and the pulse's own t0, t_end; ct: host
  * [2*size] in/out; accepted / rejected / t_final (optional) are scalars. */

@@ -50,6 +50,8 @@ struct ControlArgs {
   int mode;                   // 0: start, 1: after an attempt
   double h0, dt_max;
   int max_attempts;
+  FixedStep fx;               // fixed-step mode (the reference's semantics)
+  unsigned* status;
 };
 
 // The next attempt's step: h capped at the time left (the final step lands
@@ -58,6 +60,11 @@ __device__ void prepare_step(const ControlArgs& a, int q) {
   const ColState& c = a.c;
   if (c.done[q]) {
     c.hatt[q] = 0.0;
+    return;
+  }
+  if (a.fx.on) {  // one step of dt; the pulse ends after nsteps of them
+    c.hatt[q] = a.fx.dt;
+    c.last[q] = (c.nacc[q] + 1 >= c.nsteps[q]) ? 1 : 0;
     return;
   }
   double h = c.h[q];
@@ -92,7 +99,42 @@ __global__ void k_batch_control(const __grid_constant__ ControlArgs a) {
   const int q = (blockIdx.x * blockDim.x + threadIdx.x) / kCtlLanes;
   const int lane = threadIdx.x % kCtlLanes;
   const ColState& c = a.c;
-  if (q < a.ncol && lane == 0) {
+  if (q < a.ncol && lane == 0 && a.fx.on) {
+    // fixed-step mode: accept every step whose norm is finite, t += dt as the
+    // reference's loop does, retire after nsteps steps
+    if (a.mode == 0) {
+      c.h[q] = a.fx.dt;
+      c.done[q] = (c.nsteps[q] <= 0) ? 1 : 0;
+      c.accepted[q] = 0;
+      c.retired[q] = 0;
+      a.err[q] = 0ull;
+      if (c.done[q]) retire(a, q);
+      prepare_step(a, q);
+    } else {
+      c.accepted[q] = 0;
+      if (!c.done[q]) {
+        a.err[q] = 0ull;
+        double ns = 0.0;
+        for (int r = 0; r < a.nrowtiles; ++r) ns += a.normpart[(long long)r * a.ldc + q];
+        const double nrm = sqrt(ns);
+        c.natt[q] += 1;
+        if (nrm > 0.0 && isfinite(nrm)) {
+          c.t[q] = c.t[q] + a.fx.dt;
+          c.nacc[q] += 1;
+          c.accepted[q] = 1;
+          c.nrm[q] = nrm;
+          if (a.fx.norm_hist)
+            a.fx.norm_hist[(long long)c.pulse_id[q] * a.fx.hist_ld + c.nacc[q] - 1] = nrm;
+          if (c.nacc[q] >= c.nsteps[q]) c.done[q] = 1;
+        } else {
+          atomicOr(a.status, ST_NONFINITE);
+          c.done[q] = 2;
+        }
+        if (c.done[q]) retire(a, q);
+        prepare_step(a, q);
+      }
+    }
+  } else if (q < a.ncol && lane == 0) {
     if (a.mode == 0) {
       c.h[q] = a.h0;
       c.done[q] = (c.t[q] >= c.t_end[q]) ? 1 : 0;
@@ -145,7 +187,9 @@ __global__ void k_batch_control(const __grid_constant__ ControlArgs a) {
   }
   __syncthreads();
   if (q < a.ncol && lane < kNumStages) {
-    const double F = c.done[q] ? 0.0 : dev_field(c.pulse[q], c.t[q] + c_C[lane] * c.hatt[q]);
+    // stage fields F(t + c_s h); in fixed-step mode F(t + dt) for every stage
+    const double ts = a.fx.on ? c.t[q] + a.fx.dt : c.t[q] + c_C[lane] * c.hatt[q];
+    const double F = c.done[q] ? 0.0 : dev_field(c.pulse[q], ts);
     a.Fs[lane * a.ldc + q] = F;
   }
 }
@@ -156,6 +200,7 @@ struct ApplyArgs {
   ColState c;
   double2* out;     // [B][n] final states (user layout)
   int ntot, ncol, ldc;
+  FixedStep fx;     // fixed-step mode: the population history
 };
 
 __global__ void k_batch_apply(const __grid_constant__ ApplyArgs a) {
@@ -172,6 +217,9 @@ __global__ void k_batch_apply(const __grid_constant__ ApplyArgs a) {
     const double nrm = a.c.nrm[q];
     o = make_double2(v.x / nrm, v.y / nrm);
     a.X[idx] = o;
+    if (a.fx.pop_hist && i == a.fx.pop_index)
+      a.fx.pop_hist[(long long)a.c.pulse_id[q] * a.fx.hist_ld + a.c.nacc[q]] =
+          __dadd_rn(__dmul_rn(o.x, o.x), __dmul_rn(o.y, o.y));
   } else {
     if (!a.c.retired[q]) return;
     o = a.X[idx];
@@ -285,6 +333,7 @@ int ensure_batch(mpc_ctx* c, int B) {
       (rc = balloc(b, &s.nacc, ldc)) || (rc = balloc(b, &s.nrej, ldc)) ||
       (rc = balloc(b, &s.natt, ldc)) || (rc = balloc(b, &s.pulse_id, ldc)) ||
       (rc = balloc(b, &s.nrm, ldc)) || (rc = balloc(b, &s.retired, ldc)) ||
+      (rc = balloc(b, &s.nsteps, ldc)) ||
       (rc = balloc(b, &b->res.nacc, ldc)) || (rc = balloc(b, &b->res.nrej, ldc)) ||
       (rc = balloc(b, &b->res.t, ldc)) || (rc = balloc(b, &b->res.status, ldc)))
     return rc;
@@ -456,18 +505,16 @@ int mpc_batch_autotune(mpc_ctx* c, int B, double* table, int cap) {
   return rows;
 }
 
-int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0,
-                        const double* t_end, double h0, double dt_max, double rtol, double atol,
-                        int max_attempts, double* ct, int* accepted, int* rejected,
-                        double* t_final) {
-  if (!c || !pulses || !t0 || !t_end || !ct || B <= 0)
-    return mpc_fail(MPC_ERR_ARG, "bad argument");
-  if (!(h0 > 0.0) || !(dt_max > 0.0) || !(rtol >= 0.0) || !(atol >= 0.0) || rtol + atol <= 0.0)
-    return mpc_fail(MPC_ERR_ARG, "bad step-control parameters");
-  if (h0 * c->eps_max > kRk78ImagStability * 4.0 || dt_max * c->eps_max > kRk78ImagStability)
-    return mpc_fail(MPC_ERR_UNSTABLE,
-                    "dt_max*max|E| = %.4g exceeds the RKF78 imaginary-axis stability bound %.4g",
-                    dt_max * c->eps_max, kRk78ImagStability);
+}  // extern "C"
+
+namespace {
+
+// The batched driver shared by the adaptive entry point and the fixed-step
+// one (fx->on: the reference's semantics; nsteps[B] the per-pulse step
+// counts, t_end unused).
+int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, const double* t_end,
+              double h0, double dt_max, double rtol, double atol, int max_attempts, double* ct,
+              int* accepted, int* rejected, double* t_final, FixedStep fx, const int* nsteps) {
   CK(cudaSetDevice(c->device));
   int rc;
   if ((rc = ensure_batch(c, B))) return rc;
@@ -487,6 +534,8 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
   CK(cudaMemcpyAsync(s.nacc, zeros.data(), sizeof(int) * B, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(s.nrej, zeros.data(), sizeof(int) * B, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(s.natt, zeros.data(), sizeof(int) * B, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(s.nsteps, fx.on ? nsteps : zeros.data(), sizeof(int) * B,
+                     cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(b->out, ct, sizeof(double2) * (size_t)n * B, cudaMemcpyHostToDevice,
                      c->stream));
   k_batch_load<<<blocks_for((long long)n * B, 256), 256, 0, c->stream>>>(b->X, b->out, n, B, ldc);
@@ -503,6 +552,8 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
   ca.h0 = h0;
   ca.dt_max = dt_max;
   ca.max_attempts = max_attempts > 0 ? max_attempts : 1000000000;
+  ca.fx = fx;
+  ca.status = c->d_status;
   ApplyArgs aa{};
   aa.X = b->X;
   aa.Xn = b->Y[1];
@@ -510,6 +561,7 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
   aa.out = b->out;
   aa.ntot = n;
   aa.ldc = ldc;
+  aa.fx = fx;
 
   int ncol = B;
   ca.ncol = ncol;
@@ -577,6 +629,7 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
     GATHER(pulse_id, int)
     GATHER(nrm, double)
     GATHER(retired, int)
+    GATHER(nsteps, int)
     for (int st = 0; st < kNumStages; ++st) {
       k_gather_scalar<double><<<sb, 128, 0, c->stream>>>(reinterpret_cast<double*>(b->scratch),
                                                          b->Fs + st * ldc, b->map, act);
@@ -678,6 +731,7 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
       l.rtol = rtol;
       l.atol = atol;
       l.dt_max = dt_max;
+      l.fx = fx;
       while (true) {
         int P = 1;
         while (P < ncol) P *= 2;
@@ -714,9 +768,107 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
     gave_up += stt[i] == 2;
   }
   if (gave_up)
-    return mpc_fail(MPC_ERR_DEVICE, "%d pulse(s) stopped after max_attempts step attempts",
+    return mpc_fail(MPC_ERR_DEVICE,
+                    fx.on ? "%d pulse(s) stopped on a non-finite norm"
+                          : "%d pulse(s) stopped after max_attempts step attempts",
                     gave_up);
   return MPC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0,
+                        const double* t_end, double h0, double dt_max, double rtol, double atol,
+                        int max_attempts, double* ct, int* accepted, int* rejected,
+                        double* t_final) {
+  if (!c || !pulses || !t0 || !t_end || !ct || B <= 0)
+    return mpc_fail(MPC_ERR_ARG, "bad argument");
+  if (!(h0 > 0.0) || !(dt_max > 0.0) || !(rtol >= 0.0) || !(atol >= 0.0) || rtol + atol <= 0.0)
+    return mpc_fail(MPC_ERR_ARG, "bad step-control parameters");
+  if (h0 * c->eps_max > kRk78ImagStability * 4.0 || dt_max * c->eps_max > kRk78ImagStability)
+    return mpc_fail(MPC_ERR_UNSTABLE,
+                    "dt_max*max|E| = %.4g exceeds the RKF78 imaginary-axis stability bound %.4g",
+                    dt_max * c->eps_max, kRk78ImagStability);
+  FixedStep fx{};
+  return batch_run(c, B, pulses, t0, t_end, h0, dt_max, rtol, atol, max_attempts, ct, accepted,
+                   rejected, t_final, fx, nullptr);
+}
+
+int mpc_batch_advance(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, double dt,
+                      const int* steps, int pop_index, double* ct, double* pop_out,
+                      double* norm_out) {
+  if (!c || !pulses || !t0 || !steps || !ct || B <= 0)
+    return mpc_fail(MPC_ERR_ARG, "bad argument");
+  if (!(dt > 0.0)) return mpc_fail(MPC_ERR_ARG, "dt must be > 0");
+  if (pop_index < 0 || pop_index >= c->g.ntot) return mpc_fail(MPC_ERR_ARG, "pop_index out of range");
+  int max_steps = 0;
+  for (int b = 0; b < B; ++b) {
+    if (steps[b] < 0) return mpc_fail(MPC_ERR_ARG, "steps[%d] < 0", b);
+    max_steps = std::max(max_steps, steps[b]);
+  }
+  if (dt * c->eps_max > kRk78ImagStability)
+    return mpc_fail(MPC_ERR_UNSTABLE,
+                    "dt*max|E| = %.4g exceeds the RKF78 imaginary-axis stability bound %.4g",
+                    dt * c->eps_max, kRk78ImagStability);
+  CK(cudaSetDevice(c->device));
+  FixedStep fx{};
+  fx.on = 1;
+  fx.dt = dt;
+  fx.pop_index = pop_index;
+  fx.hist_ld = (long long)max_steps + 1;
+  double* dpop = nullptr;
+  double* dnrm = nullptr;
+  auto release = [&]() {
+    if (dpop) cudaFree(dpop);
+    if (dnrm) cudaFree(dnrm);
+  };
+  if (pop_out && cudaMalloc(&dpop, sizeof(double) * (size_t)B * fx.hist_ld) != cudaSuccess) {
+    cudaGetLastError();
+    return mpc_fail(MPC_ERR_NOMEM, "population history of %d x %lld", B, fx.hist_ld);
+  }
+  if (norm_out && cudaMalloc(&dnrm, sizeof(double) * (size_t)B * fx.hist_ld) != cudaSuccess) {
+    cudaGetLastError();
+    release();
+    return mpc_fail(MPC_ERR_NOMEM, "norm history of %d x %lld", B, fx.hist_ld);
+  }
+  fx.pop_hist = dpop;
+  fx.norm_hist = dnrm;
+  std::vector<double> t_end(B), pop0(B);
+  for (int b = 0; b < B; ++b) {
+    t_end[b] = t0[b] + steps[b] * dt;
+    // entry 0 of the history: the start state, as the reference writes it
+    // before its loop
+    const double* x = ct + 2 * (size_t)b * c->g.ntot + 2 * (size_t)pop_index;
+    pop0[b] = x[0] * x[0] + x[1] * x[1];
+  }
+  // the error-norm tolerances are unused in fixed-step mode (every finite
+  // step is accepted); 1 keeps the stage epilogue's ratio finite
+  int rc = batch_run(c, B, pulses, t0, t_end.data(), dt, dt, 1.0, 1.0, 0, ct, nullptr, nullptr,
+                     nullptr, fx, steps);
+  if (rc == MPC_OK && (dpop || dnrm)) {
+    std::vector<double> h((size_t)B * fx.hist_ld);
+    const size_t ld = (size_t)fx.hist_ld;
+    if (dpop) {
+      if (cudaMemcpy(h.data(), dpop, sizeof(double) * h.size(), cudaMemcpyDeviceToHost) !=
+          cudaSuccess)
+        rc = mpc_fail(MPC_ERR_CUDA, "history copy failed");
+      for (int b = 0; rc == MPC_OK && b < B; ++b) {
+        pop_out[b * ld] = pop0[b];
+        for (int k = 1; k <= steps[b]; ++k) pop_out[b * ld + k] = h[b * ld + k];
+      }
+    }
+    if (dnrm && rc == MPC_OK) {
+      if (cudaMemcpy(h.data(), dnrm, sizeof(double) * h.size(), cudaMemcpyDeviceToHost) !=
+          cudaSuccess)
+        rc = mpc_fail(MPC_ERR_CUDA, "history copy failed");
+      for (int b = 0; rc == MPC_OK && b < B; ++b)
+        for (int k = 0; k < steps[b]; ++k) norm_out[b * (ld - 1) + k] = h[b * ld + k];
+    }
+  }
+  release();
+  return rc;
 }
 
 }  // extern "C"

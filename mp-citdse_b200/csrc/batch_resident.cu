@@ -72,6 +72,7 @@ struct BrArgs {
   int ldc, ncol, ntot;
   int exit_below, max_attempts, gauge;
   double rtol, atol, dt_max;
+  FixedStep fx;       // fixed-step mode (the reference's semantics)
   BarrierCfg bc;
   Geometry g;
 };
@@ -137,7 +138,7 @@ __global__ void __launch_bounds__(QT, 1) k_batch_res(const __grid_constant__ BrA
   __shared__ double s_t[P], s_tend[P], s_h[P], s_hatt[P], s_nrm[P], s_nsum[P], s_err[P];
   __shared__ double s_F[kNumStages][P];
   __shared__ int s_last[P], s_done[P], s_acc[P], s_nacc[P], s_nrej[P], s_natt[P], s_pid[P],
-      s_ret[P];
+      s_ret[P], s_nsteps[P];
   __shared__ int s_exit, s_dead;
 
   // ---- coupling rows, once ----
@@ -170,12 +171,14 @@ __global__ void __launch_bounds__(QT, 1) k_batch_res(const __grid_constant__ BrA
       s_nrej[q] = a.c.nrej[q];
       s_natt[q] = a.c.natt[q];
       s_pid[q] = a.c.pulse_id[q];
+      s_nsteps[q] = a.c.nsteps[q];
     } else {
       s_pulse[q] = mpc_pulse{};
       s_t[q] = s_tend[q] = s_h[q] = 0.0;
       s_done[q] = 3;  // padding column
       s_nacc[q] = s_nrej[q] = s_natt[q] = 0;
       s_pid[q] = -1;
+      s_nsteps[q] = 0;
     }
     s_nrm[q] = 1.0;
     s_hatt[q] = 0.0;
@@ -208,6 +211,9 @@ __global__ void __launch_bounds__(QT, 1) k_batch_res(const __grid_constant__ BrA
       const int q = tid;
       if (s_done[q]) {
         s_hatt[q] = 0.0;
+      } else if (a.fx.on) {  // one step of dt
+        s_hatt[q] = a.fx.dt;
+        s_last[q] = (s_nacc[q] + 1 >= s_nsteps[q]) ? 1 : 0;
       } else {
         double h = s_h[q];
         const double rem = s_tend[q] - s_t[q];
@@ -223,7 +229,9 @@ __global__ void __launch_bounds__(QT, 1) k_batch_res(const __grid_constant__ BrA
     __syncthreads();
     for (int e = tid; e < kNumStages * P; e += QT) {
       const int s = e / P, q = e % P;
-      s_F[s][q] = s_done[q] ? 0.0 : dev_field(s_pulse[q], s_t[q] + q_C[s] * s_hatt[q]);
+      // F(t + c_s h); in fixed-step mode F(t + dt) frozen for every stage
+      const double ts = a.fx.on ? s_t[q] + a.fx.dt : s_t[q] + q_C[s] * s_hatt[q];
+      s_F[s][q] = s_done[q] ? 0.0 : dev_field(s_pulse[q], ts);
     }
     __syncthreads();
 
@@ -396,7 +404,29 @@ __global__ void __launch_bounds__(QT, 1) k_batch_res(const __grid_constant__ BrA
       }
     }
     __syncthreads();
-    if (tid < P) {
+    if (tid < P && a.fx.on) {
+      // fixed-step mode: accept every finite step, t += dt, retire after
+      // nsteps steps
+      const int q = tid;
+      s_acc[q] = 0;
+      if (!s_done[q]) {
+        const double nrm = sqrt(s_nsum[q]);
+        s_natt[q] += 1;
+        if (nrm > 0.0 && isfinite(nrm)) {
+          s_t[q] = s_t[q] + a.fx.dt;
+          s_nacc[q] += 1;
+          s_acc[q] = 1;
+          s_nrm[q] = nrm;
+          if (cta == 0 && a.fx.norm_hist)
+            a.fx.norm_hist[(long long)s_pid[q] * a.fx.hist_ld + s_nacc[q] - 1] = nrm;
+          if (s_nacc[q] >= s_nsteps[q]) s_done[q] = 1;
+        } else {
+          if (cta == 0) atomicOr(a.status, ST_NONFINITE);
+          s_done[q] = 2;
+        }
+        s_ret[q] = s_done[q] ? 1 : 0;
+      }
+    } else if (tid < P) {
       const int q = tid;
       s_acc[q] = 0;
       if (!s_done[q]) {
@@ -433,6 +463,14 @@ __global__ void __launch_bounds__(QT, 1) k_batch_res(const __grid_constant__ BrA
       }
     }
     __syncthreads();
+    // fixed-step population history: the CTA owning pop_index
+    if (a.fx.pop_hist && tid < P && s_acc[tid] && a.fx.pop_index >= row0 &&
+        a.fx.pop_index < row0 + nrows) {
+      const double2 v =
+          scaled(__ldcg(a.XN + (long long)a.fx.pop_index * ldc + tid), s_nrm[tid]);
+      a.fx.pop_hist[(long long)s_pid[tid] * a.fx.hist_ld + s_nacc[tid]] =
+          __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y));
+    }
     // pulses that finished: final state out (own rows), counters by CTA 0
     for (int e = tid; e < nrows * P; e += QT) {
       const int li = e / P, q = e % P;
@@ -641,6 +679,7 @@ int mpc_batch_res_run(mpc_ctx* c, const BatchResLaunch& l, int P, int exit_below
   a.rtol = l.rtol;
   a.atol = l.atol;
   a.dt_max = l.dt_max;
+  a.fx = l.fx;
   a.bc = mpc_barrier_cfg(c);
   a.g = c->g;
   CK(cudaMemsetAsync(r->bar, 0, sizeof(unsigned) * 2, c->stream));  // arrival counter

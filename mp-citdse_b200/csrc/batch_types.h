@@ -57,6 +57,23 @@ struct ColState {
   int* pulse_id;   // column -> pulse index
   double* nrm;
   int* retired;    // set when the pulse finishes; cleared once its state is out
+  int* nsteps;     // fixed-step mode: the pulse's step count
+};
+
+// Fixed-step mode (the reference's semantics, tdse::propV / propL,
+// src/tdse/tdse.cpp:186-215): every attempt is one step of dt with the field
+// F(t + dt) frozen for the 13 stages, always accepted unless the norm is not
+// finite, then t += dt and x /= ||x||; a pulse retires after nsteps steps.
+// Optional per-pulse histories (indexed by pulse id, rows hist_ld apart):
+// pop_hist[id][k] = |x_k[pop_index]|^2 after step k (entry 0 is the host's),
+// norm_hist[id][k-1] = ||x_new|| before the renormalisation of step k.
+struct FixedStep {
+  int on;
+  double dt;
+  int pop_index;
+  long long hist_ld;
+  double* pop_hist;
+  double* norm_hist;
 };
 
 // Per-pulse results, indexed by pulse id (columns move; these do not).
@@ -80,6 +97,7 @@ struct BatchResLaunch {
   int ncol;
   int max_attempts;
   double rtol, atol, dt_max;
+  FixedStep fx;
 };
 
 }  // namespace mpc

@@ -119,6 +119,8 @@ def lib():
     L.mpc_adjoint.argtypes = L.mpc_objective_gradient.argtypes
     L.mpc_launch_count.restype = C.c_longlong
     L.mpc_launch_count.argtypes = [C.c_void_p]
+    L.mpc_batch_advance.argtypes = [C.c_void_p, C.c_int, C.POINTER(Pulse), _dp, C.c_double, _ip,
+                                    C.c_int, _dp, _dp, _dp]
     L.mpc_ctx_set_wait_limit.argtypes = [C.c_void_p, C.c_double]
     L.mpc_ctx_inject_barrier_timeout.argtypes = [C.c_void_p]
     _lib = L
@@ -309,6 +311,27 @@ class Context:
                                          atol, int(max_attempts), _ptr(xf), acc.ctypes.data_as(_ip),
                                          rej.ctypes.data_as(_ip), _ptr(tf)))
         return xf.view(np.complex128).reshape(B, -1), acc, rej, tf
+
+    def batch_advance(self, pulses, t0, dt, steps, X, pop_index=0, history=False):
+        """Fixed-step propagation of B pulses at once with the reference's
+        semantics (mpc_batch_advance).  pulses: list of Pulse; t0, steps: [B];
+        X: [B, size] complex start states.  Returns X_final, or with
+        history=True (X_final, pop [B, M+1], norm [B, M]), M = max(steps)."""
+        B = len(pulses)
+        arr = (Pulse * B)(*pulses)
+        t0 = np.ascontiguousarray(np.broadcast_to(t0, (B,)), dtype=np.float64)
+        st = np.ascontiguousarray(np.broadcast_to(steps, (B,)), dtype=np.int32)
+        xf = np.ascontiguousarray(X, dtype=np.complex128).view(np.float64).reshape(B, -1).copy()
+        M = int(st.max()) if B else 0
+        pop = np.full((B, M + 1), np.nan) if history else None
+        nrm = np.full((B, max(M, 1)), np.nan) if history else None
+        _check(lib().mpc_batch_advance(self._h, B, arr, _ptr(t0), float(dt),
+                                       st.ctypes.data_as(_ip), int(pop_index), _ptr(xf),
+                                       _ptr(pop), _ptr(nrm)))
+        Xf = xf.view(np.complex128).reshape(B, -1)
+        if not history:
+            return Xf
+        return Xf, pop, nrm[:, :M]
 
     def propagate_adaptive(self, pulse, t0, t_end, x, h0=0.05, dt_max=0.2, rtol=1e-10,
                            atol=1e-10, max_attempts=0):

@@ -1,13 +1,26 @@
 """Writes the golden fixtures in this folder from the reference's own code.
 
 Run in a checkout where the reference source tree is present:
-    make -f oracle/Makefile && python tests/golden/make_golden.py
+    make -f oracle/Makefile REF=<reference tree> && python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --long    # the benchmark-size pulses
 
 Every number here comes from oracle/_ref/libref_tdse.so, i.e. the
 reference's src/tdse/tdse.cpp (MatVecV / MatVecL, tdse::propV / propL) and
 src/tdse/pulse.cpp compiled as they are, with only the missing third-party
 pieces stood in (odeint's RKF78 step, a CBLAS).  Inputs are small seeded
-synthetic systems in the reference's layout.
+synthetic systems in the reference's layout, and (--long) the benchmark's
+1e hydrogen system from the structure restatement:
+  cfg0_h1e.npz   one whole 10-cycle 800 nm 1e14 W/cm^2 pulse (11,032 steps,
+                 dt 0.1, length gauge) through tdse::propL: final populations,
+                 the _pop column and the _field column;
+  batch_h1e.npz  16 pulses drawn as the batched workload draws them
+                 (seed 0: intensity log-uniform 1e13-5e14 W/cm^2, 400-1600
+                 nm, 4-20 cycles; CEP 0, which is what the reference's main
+                 passes), each a whole pulse through propL at dt 0.05: final
+                 populations and every 100th entry of each _pop column.
+Both also keep a fingerprint of the system (energies, per-block Frobenius
+norms of the dipoles) so that a test can check that it rebuilt the same
+system before comparing.
 """
 import os
 import sys
@@ -76,5 +89,72 @@ def main():
     print("golden fixtures written to", HERE)
 
 
+def h1e_system():
+    from mpc_tdse.structure1e import hydrogen
+
+    return hydrogen(n=300, k=9, R=200.0, l_max=5, gauge="l", states=[292] * 6)
+
+
+def fingerprint(s):
+    return s.eig.copy(), np.array([np.linalg.norm(s.block(L)) for L in range(len(s.n) - 1)])
+
+
+def batch_pulse_params(B=16, seed=0):
+    """(Io W/cm^2, photon energy eV, cycles) of the first B pulses of the
+    batched workload's seeded draw (the same generator calls as bench.py)."""
+    rng = np.random.default_rng(seed)
+    n_all = 256
+    Io = 10 ** rng.uniform(13, np.log10(5e14), n_all)
+    lam = rng.uniform(400, 1600, n_all)
+    rng.uniform(0, 2 * np.pi, n_all)   # CEP draw (the reference's main uses 0)
+    cyc = rng.integers(4, 21, n_all)
+    return [(float(Io[i]), 1239.84198 / float(lam[i]), int(cyc[i])) for i in range(B)]
+
+
+def _one_pulse(job):
+    """One whole pulse through the reference's propL on a single host thread
+    (run in a process pool)."""
+    Io, w_eV, cycles, dt = job
+    ref = Reference()
+    ref.use_openblas(1)
+    s = h1e_system()
+    x0 = np.zeros(s.ntot, complex)
+    x0[0] = 1.0
+    steps = ref.steps(w_eV, cycles, 0.0, dt)
+    with tempfile.TemporaryDirectory() as d:
+        ct = ref.propagate(s.n, s.eig, s.dip, "l", "sine", Io, w_eV, cycles, 0.0, dt, steps,
+                           x0, os.path.join(d, "h"))
+        pop = np.loadtxt(os.path.join(d, "h_pop10.dat"))
+        fld = np.loadtxt(os.path.join(d, "h_field.dat"))
+    return steps, np.abs(ct) ** 2, pop, fld
+
+
+def main_long():
+    import multiprocessing as mp
+
+    s = h1e_system()
+    eig, dnorm = fingerprint(s)
+    jobs = [(1e14, 1.5498, 10, 0.1)] + [(Io, w, c, 0.05) for Io, w, c in batch_pulse_params()]
+    with mp.get_context("spawn").Pool(min(len(jobs), os.cpu_count() or 1)) as pool:
+        res = pool.map(_one_pulse, jobs)
+    steps, pops, pop, fld = res[0]
+    np.savez_compressed(os.path.join(HERE, "cfg0_h1e.npz"), steps=np.array(steps), pops=pops,
+                        pop=pop, field=fld, eig=eig, dnorm=dnorm,
+                        pulse=np.array([1e14, 1.5498, 10, 0.1]))
+    out = {"eig": eig, "dnorm": dnorm, "dt": np.array(0.05),
+           "params": np.array([j[:3] for j in jobs[1:]])}
+    for b, (steps, pops, pop, _) in enumerate(res[1:]):
+        out[f"steps_{b}"] = np.array(steps)
+        out[f"pops_{b}"] = pops
+        idx = np.unique(np.concatenate([np.arange(0, steps + 1, 100), [steps]]))
+        out[f"popidx_{b}"] = idx
+        out[f"pop_{b}"] = pop[idx, 1]
+    np.savez_compressed(os.path.join(HERE, "batch_h1e.npz"), **out)
+    print("benchmark-size fixtures written to", HERE)
+
+
 if __name__ == "__main__":
-    main()
+    if "--long" in sys.argv:
+        main_long()
+    else:
+        main()

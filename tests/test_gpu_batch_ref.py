@@ -1,0 +1,174 @@
+"""Parity of the reference-semantics paths at the benchmark's sizes, and of
+the batched fixed-step path (mpc_batch_advance) with the reference's own
+propagation loop.
+
+* Batched fixed step vs oracle/_ref: pulses of different lengths, batched,
+  each compared with the reference's tdse::propL / propV (src/tdse/tdse.cpp
+  :186-215, built from its own source) run alone: final populations and the
+  _pop column within 1e-9, on both batched paths (stage GEMM with the
+  resident tail, and stage GEMM only).
+* Benchmark sizes, against fixtures made by the reference's own code
+  (tests/golden/make_golden.py --long) on the benchmark's 1e hydrogen system
+  (300 B-splines, R = 200, the 292 states per l below 20 a.u., l = 0..5):
+  - one whole 10-cycle 800 nm 1e14 W/cm^2 pulse (11,032 steps at dt 0.1) on
+    both single-pulse paths: final populations, the _pop column and the PES
+    of the final state within 1e-9, the _field column to its 6 printed digits;
+  - 16 pulses drawn as the batched workload draws them (intensity up to
+    5e14 W/cm^2, 400-1600 nm, 4-20 cycles, CEP 0), dt 0.05, batched: final
+    populations and the _pop column within 1e-9.
+  The system is rebuilt here by the structure restatement; its fingerprint
+  (energies, dipole block norms) is checked against the fixture's first.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import mpc_tdse
+from mpc_tdse.systems import hydrogen_like_1e
+from oracle import Reference, pes_reference
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL = 1e-9
+
+
+def _ref_pulse(ref, s, gauge, shape, Io, w_eV, cycles, dt):
+    x0 = np.zeros(s.ntot, complex)
+    x0[0] = 1.0
+    steps = ref.steps(w_eV, cycles, 0.0, dt)
+    with tempfile.TemporaryDirectory() as d:
+        ct = ref.propagate(s.n, s.eig, s.dip, gauge, shape, Io, w_eV, cycles, 0.0, dt, steps, x0,
+                           os.path.join(d, "h"))
+        pop = np.loadtxt(os.path.join(d, "h_pop10.dat"))
+    return steps, ct, pop[:, 1]
+
+
+@pytest.mark.parametrize("gauge", ["l", "v"])
+@pytest.mark.parametrize("path", ["auto", "streaming"])
+def test_batch_advance_matches_reference_per_pulse(gauge, path):
+    if not Reference.available():
+        pytest.skip("reference build not present")
+    s = hydrogen_like_1e(40, 3, gauge=gauge, seed=5)
+    ref = Reference()
+    ref.use_plain_loops()
+    # 12 pulses of different intensity, colour, length and shape
+    rng = np.random.default_rng(7)
+    params = []
+    for b in range(12):
+        Io = float(10 ** rng.uniform(13, 14.5))
+        w_eV = float(1239.84198 / rng.uniform(500, 900))
+        cycles = int(rng.integers(1, 4))
+        shape = "gaussian" if b == 5 else "sine"
+        params.append((shape, Io, w_eV, cycles))
+    dt = 0.1
+    pulses, steps, refs = [], [], []
+    for shape, Io, w_eV, cycles in params:
+        Iau, wau = mpc_tdse.to_au(Io, w_eV)
+        tau = mpc_tdse.period(wau, cycles)
+        pulses.append(mpc_tdse.pulse_setup(shape, gauge, Iau, wau, 0.0, cycles, tau))
+        n, ct, pop = _ref_pulse(ref, s, gauge, shape, Io, w_eV, cycles, dt)
+        steps.append(n)
+        refs.append((ct, pop))
+    assert len(set(steps)) > 4   # uneven lengths: pulses retire at different steps
+    X0 = np.zeros((len(pulses), s.ntot), complex)
+    X0[:, 0] = 1.0
+    with mpc_tdse.Context.from_system(s) as ctx:
+        ctx.set_path(path)
+        X, pop, nrm = ctx.batch_advance(pulses, 0.0, dt, steps, X0, pop_index=0, history=True)
+    for b, (ct, pref) in enumerate(refs):
+        assert np.max(np.abs(np.abs(X[b]) ** 2 - np.abs(ct) ** 2)) < TOL, b
+        assert np.max(np.abs(pop[b, :steps[b] + 1] - pref)) < TOL, b
+        assert np.max(np.abs(nrm[b, :steps[b]] - 1.0)) < 1e-8, b
+
+
+def test_batch_advance_equals_single_pulse_path():
+    s = hydrogen_like_1e(30, 2, gauge="v", seed=2)
+    Iau, wau = mpc_tdse.to_au(2e14, 1.5498)
+    pulses, steps = [], []
+    for cyc in (1, 2, 3):
+        tau = mpc_tdse.period(wau, cyc)
+        pulses.append(mpc_tdse.pulse_setup("sine", "v", Iau * cyc / 3, wau, 0.0, cyc, tau))
+        steps.append(int(tau / 0.1))
+    X0 = np.zeros((3, s.ntot), complex)
+    X0[:, 0] = 1.0
+    with mpc_tdse.Context.from_system(s) as ctx:
+        X, pop, nrm = ctx.batch_advance(pulses, 0.0, 0.1, steps, X0, history=True)
+        for b in range(3):
+            ct, p1, _, n1 = ctx.propagate(pulses[b], 0.0, 0.1, steps[b], X0[b])
+            assert np.max(np.abs(X[b] - ct)) < 1e-11
+            assert np.max(np.abs(pop[b, :steps[b] + 1] - p1)) < 1e-12
+            assert np.max(np.abs(nrm[b, :steps[b]] - n1)) < 1e-12
+
+
+def _h1e_system(fx):
+    from mpc_tdse.structure1e import hydrogen
+
+    s = hydrogen(n=300, k=9, R=200.0, l_max=5, gauge="l", states=[292] * 6)
+    dn = np.array([np.linalg.norm(s.block(L)) for L in range(len(s.n) - 1)])
+    assert np.max(np.abs(s.eig - fx["eig"]) / np.maximum(1.0, np.abs(fx["eig"]))) < 1e-10
+    assert np.max(np.abs(dn - fx["dnorm"]) / fx["dnorm"]) < 1e-10
+    return s
+
+
+@pytest.mark.parametrize("path", ["streaming", "resident"])
+def test_cfg0_whole_pulse_matches_reference(path):
+    """a whole 11,032-step pulse on 1752 states."""
+    fx = np.load(os.path.join(GOLDEN, "cfg0_h1e.npz"))
+    s = _h1e_system(fx)
+    Io, w_eV, cycles, dt = fx["pulse"]
+    steps = int(fx["steps"])
+    Iau, wau = mpc_tdse.to_au(Io, w_eV)
+    tau = mpc_tdse.period(wau, int(cycles))
+    p = mpc_tdse.pulse_setup("sine", "l", Iau, wau, 0.0, int(cycles), tau)
+    x0 = np.zeros(s.ntot, complex)
+    x0[0] = 1.0
+    with mpc_tdse.Context.from_system(s) as ctx:
+        ctx.set_path(path)
+        ct, pop, fld, nrm = ctx.propagate(p, 0.0, dt, steps, x0)
+        pes, st = ctx.pes(1)
+    pops = np.abs(ct) ** 2
+    err = float(np.max(np.abs(pops - fx["pops"])))
+    drift = float(np.max(np.abs(nrm - 1.0)))
+    print(f"\nconfigs[0] {path}: {steps} steps, max |pop - reference| = {err:.2e}, "
+          f"pre-renormalisation norm drift <= {drift:.2e}")
+    assert err < TOL
+    assert np.max(np.abs(pop - fx["pop"][:, 1])) < TOL
+    # the reference prints the field with 6 significant digits
+    assert np.allclose(fld, fx["field"][:, 1], rtol=1e-5, atol=1e-9)
+    assert drift < 1e-8
+    # the PES of the final state (pes::genPES1e's binning) from the
+    # reference's populations
+    pes_r, g_r, nrm_r, y_r, _ = pes_reference(s.n, s.eig, np.sqrt(fx["pops"]), electrons=1)
+    assert np.max(np.abs(pes - pes_r)) < TOL
+    assert abs(st["ground"] - g_r) < TOL and abs(st["yield"] - y_r) < TOL
+
+
+def test_batched_workload_pulses_match_reference():
+    """16 pulses of the batched workload's draw, fixed step dt 0.05, batched."""
+    fx = np.load(os.path.join(GOLDEN, "batch_h1e.npz"))
+    s = _h1e_system(fx)
+    dt = float(fx["dt"])
+    pulses, steps = [], []
+    for b, (Io, w_eV, cycles) in enumerate(fx["params"]):
+        Iau, wau = mpc_tdse.to_au(Io, w_eV)
+        tau = mpc_tdse.period(wau, int(cycles))
+        pulses.append(mpc_tdse.pulse_setup("sine", "l", Iau, wau, 0.0, int(cycles), tau))
+        steps.append(int(fx[f"steps_{b}"]))
+    X0 = np.zeros((len(pulses), s.ntot), complex)
+    X0[:, 0] = 1.0
+    with mpc_tdse.Context.from_system(s) as ctx:
+        X, pop, nrm = ctx.batch_advance(pulses, 0.0, dt, steps, X0, history=True)
+    worst = 0.0
+    for b in range(len(pulses)):
+        e = float(np.max(np.abs(np.abs(X[b]) ** 2 - fx[f"pops_{b}"])))
+        worst = max(worst, e)
+        assert e < TOL, b
+        idx = fx[f"popidx_{b}"]
+        assert np.max(np.abs(pop[b, idx] - fx[f"pop_{b}"])) < TOL, b
+    drift = max(float(np.max(np.abs(nrm[b, :steps[b]] - 1.0))) for b in range(len(pulses)))
+    print(f"\nbatched workload, 16 pulses ({min(steps)}-{max(steps)} steps): max |pop - "
+          f"reference| = {worst:.2e}, norm drift <= {drift:.2e}")
+    assert drift < 1e-8
