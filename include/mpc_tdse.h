@@ -297,6 +297,20 @@ int mpc_batch_objective_gradient(mpc_ctx *ctx, int B, const mpc_pulse *pulses, i
 int mpc_pes(mpc_ctx *ctx, int electrons, double threshold, const double *ct, double *pes,
             int ngrid, double *stats);
 
+/* The summed spectrum of `pes -s` for the same state (src/pes/pes.cpp
+ * :127-137, :215-245): 1e, the blocks' binned spectra added per bin; 2e,
+ * every state i >= 1 of every block binned onto the L = 1 energies (first
+ * matching bin 1 <= k <= n_1 - 1, the bin's upper neighbour for k = n_1 - 1
+ * being the first L = 2 energy, as the reference indexes it; bins stop at
+ * n_1 - 2 when L_max = 1), density |c_i|^2 * 2 / (dn + dp).  grid[k]
+ * receives E1[k] (1e) or E1[k] - threshold (2e) and pes[k] the density,
+ * k < n_1 = state_sz[1]; ngrid >= n_1 (entries past n_1 are zeroed).  The
+ * reference writes the rows k <= n_1 - 2 (1e: n_0 - 2) with grid[k] > 0.
+ * The reference sizes its accumulator by state_sz[L_max] and reads one
+ * energy past block 1; here the bins have their own array of n_1. */
+int mpc_pes_summed(mpc_ctx *ctx, int electrons, double threshold, const double *ct, double *grid,
+                   double *pes, int ngrid);
+
 /* Measures the FP64 tensor-core (mma.sync .f64) and FP64 FMA throughput of
  * CUDA device `device` in TFLOP/s: the roofline denominators of the batched
  * GEMM.  Takes ~50 ms. */

@@ -283,6 +283,11 @@ struct mpc_adjoint_state {
   double2* segX = nullptr;    // [ckpt + 1][ntot]
   double2* segY = nullptr;    // [ckpt][13][ntot]  (slot 0 unused: y_0 = x_n)
   double* segN = nullptr;     // [ckpt]
+  // a second segment buffer set for the fused reverse pass (recompute of one
+  // segment while the previous one is swept), allocated on first use
+  double2* segX2 = nullptr;
+  double2* segY2 = nullptr;
+  double* segN2 = nullptr;
   double2* lam = nullptr;
   double2* zbar = nullptr;
   double2* v = nullptr;
@@ -494,7 +499,23 @@ int mpc_objective_backward(mpc_ctx* c, double* grad_u, double* dJdF) {
   ac.gauge = (c->gauge == 'l') ? 0 : 1;
   ac.h = dt;
   ac.g = c->g;
-  for (int seg = nseg - 1; seg >= 0; --seg) {
+  if (a->resident && mpc_resident_fused_ok(c)) {
+    // one persistent launch: each segment's recompute runs concurrently with
+    // the sweep of the segment after it
+    if (!a->segX2) {
+      if ((rc = aalloc(a, &a->segX2, n * (ckpt + 1))) ||
+          (rc = aalloc(a, &a->segY2, n * (size_t)ckpt * kNumStages)) ||
+          (rc = aalloc(a, &a->segN2, ckpt)))
+        return rc;
+    }
+    double2* sx[2] = {a->segX, a->segX2};
+    double2* sy[2] = {a->segY, a->segY2};
+    double* sn[2] = {a->segN, a->segN2};
+    if ((rc = mpc_resident_backward_fused(c, a->ckpts, steps, ckpt, c->d_Ftab, dt, sx, sy, sn,
+                                          a->lam, a->fbar, (long long)n)))
+      return rc;
+  }
+  for (int seg = nseg - 1; seg >= 0 && !(a->resident && mpc_resident_fused_ok(c)); --seg) {
     const int n0 = seg * ckpt;
     const int len = std::min(ckpt, steps - n0);
     if (a->resident) {

@@ -133,6 +133,13 @@ int mpc_resident_forward_ex(mpc_ctx* c, const double2* x_in, double2* x_out, con
 int mpc_resident_adjoint(mpc_ctx* c, const double* Ftab, double dt, int len,
                          const double2* seg_x, const double2* seg_y, const double* seg_n,
                          double2* lam, double* fbar, long long vpitch);
+// The fused reverse pass (recompute of one segment concurrent with the sweep
+// of the next, one persistent launch; resident.cu).
+bool mpc_resident_fused_ok(mpc_ctx* c);
+int mpc_resident_backward_fused(mpc_ctx* c, const double2* ckpts, int steps, int ckpt_every,
+                                const double* Ftab, double dt, double2* const* segX,
+                                double2* const* segY, double* const* segN, double2* lam,
+                                double* fbar, long long vpitch);
 
 // Launch helpers of the single-pulse path (mpc_tdse.cu), used by adjoint.cu.
 int mpc_launch_stream(mpc_ctx* c, const double2* y);

@@ -11,9 +11,11 @@
 // 2e (pes::genPES2e): per L, state 1 <= i <= n_L - 2 with E_i > threshold
 //   has density |c_i|^2 * 2 / (E_{i+1} - E_{i-1}) at E_i - threshold and adds
 //   to the yield; every such state except the global ground state adds to
-//   the excited population; the summed spectrum bins onto the L = 1 energies
-//   as in 1e (bins 1 <= k <= n1 - 1, whose upper neighbour for k = n1 - 1 is
-//   the first energy of L = 2, as the reference indexes it).
+//   the excited population.  The summed spectrum (pes -s, mpc_pes_summed)
+//   bins every state i >= 1 of every block onto the L = 1 energies as in 1e
+//   (bins 1 <= k <= n1 - 1, whose upper neighbour for k = n1 - 1 is the first
+//   energy of L = 2, as the reference indexes its concatenated energies; with
+//   L_max = 1 there is no such energy and the bins stop at n1 - 2).
 // Sums run in a fixed order (one thread per bin or state, then one CTA), so
 // results repeat bit for bit.
 #include <cuda_runtime.h>
@@ -137,7 +139,86 @@ __global__ void k_pes_stats(const __grid_constant__ PesArgs a) {
   }
 }
 
+// The summed spectrum, one thread per bin k of the L = 1 grid.  Per bin the
+// states are visited in the reference's order (block by block, state by
+// state); the bins are disjoint intervals, so a state's first matching bin
+// is its only one.
+__global__ void k_pes_summed(const __grid_constant__ PesArgs a, double* grid, int n1) {
+  const Geometry& g = a.g;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n1) return;
+  const double* E1 = a.eps + g.state_off[1];
+  double out = 0.0;
+  if (a.electrons == 1) {
+    const int n0 = g.state_off[1] - g.state_off[0];
+    if (k >= 1 && k <= n0 - 2) {
+      const double dn = fabs(E1[k] - E1[k - 1]), dp = fabs(E1[k + 1] - E1[k]);
+      const double lo = E1[k] - 0.5 * dn, hi = E1[k] + 0.5 * dp;
+      for (int L = 0; L < g.nstate_blk; ++L) {  // the block's spectrum, then the sum
+        const int o = g.state_off[L], nL = g.state_off[L + 1] - o;
+        double pl = 0.0;
+        for (int i = 1; i < nL; ++i) {
+          const double e = a.eps[o + i];
+          if (e > lo && e < hi) pl += nsq(a.c[o + i]) * 2.0 / (dn + dp);
+        }
+        out += pl;
+      }
+    }
+    grid[k] = E1[k];
+  } else {
+    const int kmax = g.nstate_blk > 2 ? n1 - 1 : n1 - 2;
+    if (k >= 1 && k <= kmax) {
+      // E1[k + 1] is the first L = 2 energy for k = n1 - 1 (contiguous eps)
+      const double dn = fabs(E1[k] - E1[k - 1]), dp = fabs(E1[k + 1] - E1[k]);
+      const double lo = E1[k] - 0.5 * dn, hi = E1[k] + 0.5 * dp;
+      for (int L = 0; L < g.nstate_blk; ++L) {
+        const int o = g.state_off[L], nL = g.state_off[L + 1] - o;
+        for (int i = 1; i < nL; ++i) {
+          const double e = a.eps[o + i];
+          if (e > lo && e < hi) out += nsq(a.c[o + i]) * 2.0 / (dn + dp);
+        }
+      }
+    }
+    grid[k] = E1[k] - a.threshold;
+  }
+  a.pes[k] = out;
+}
+
 }  // namespace
+
+extern "C" int mpc_pes_summed(mpc_ctx* c, int electrons, double threshold, const double* ct,
+                              double* grid, double* pes, int ngrid) {
+  if (!c || !grid || !pes || (electrons != 1 && electrons != 2))
+    return mpc_fail(MPC_ERR_ARG, "bad argument");
+  const Geometry& g = c->g;
+  if (g.nstate_blk < 2) return mpc_fail(MPC_ERR_ARG, "the summed spectrum needs block 1");
+  const int n1 = g.state_off[2] - g.state_off[1];
+  if (ngrid < n1) return mpc_fail(MPC_ERR_ARG, "ngrid must be at least n_1 (%d)", n1);
+  CK(cudaSetDevice(c->device));
+  double *d_pes = nullptr, *d_grid = nullptr;
+  CK(cudaMallocAsync(&d_pes, sizeof(double) * n1, c->stream));
+  CK(cudaMallocAsync(&d_grid, sizeof(double) * n1, c->stream));
+  if (ct)
+    CK(cudaMemcpyAsync(c->d_y, ct, sizeof(double2) * g.ntot, cudaMemcpyHostToDevice, c->stream));
+  PesArgs a{};
+  a.c = ct ? c->d_y : c->d_x;
+  a.eps = c->d_eps;
+  a.pes = d_pes;
+  a.electrons = electrons;
+  a.threshold = threshold;
+  a.ngrid = n1;
+  a.g = g;
+  k_pes_summed<<<(n1 + 127) / 128, 128, 0, c->stream>>>(a, d_grid, n1);
+  CK(cudaGetLastError());
+  c->launches += 1;
+  CK(cudaMemcpyAsync(pes, d_pes, sizeof(double) * n1, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(grid, d_grid, sizeof(double) * n1, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaFreeAsync(d_pes, c->stream));
+  CK(cudaFreeAsync(d_grid, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int k = n1; k < ngrid; ++k) pes[k] = grid[k] = 0.0;
+  return MPC_OK;
+}
 
 extern "C" int mpc_pes(mpc_ctx* c, int electrons, double threshold, const double* ct, double* pes,
                        int ngrid, double* stats) {

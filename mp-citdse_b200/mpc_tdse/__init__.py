@@ -108,6 +108,7 @@ def lib():
                                          _dp, _ip, _ip, _dp]
     L.mpc_probe_fp64_peak.argtypes = [C.c_int, _dp, _dp]
     L.mpc_pes.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp, C.c_int, _dp]
+    L.mpc_pes_summed.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp, _dp, C.c_int]
     L.mpc_ctx_set_path.argtypes = [C.c_void_p, C.c_int]
     L.mpc_ctx_get_path.argtypes = [C.c_void_p]
     L.mpc_objective.argtypes = [C.c_void_p, C.POINTER(Pulse), C.c_int, _dp, C.c_double, C.c_double,
@@ -355,6 +356,15 @@ class Context:
         _check(lib().mpc_pes(self._h, int(electrons), float(threshold), _ptr(cf), _ptr(out), ngrid,
                              _ptr(st)))
         return out, {"ground": st[0], "norm": st[1], "yield": st[2], "excited": st[3]}
+
+    def pes_summed(self, electrons=1, threshold=0.0, ct=None):
+        """(grid [n_1], pes [n_1]): the summed spectrum of `pes -s`."""
+        n1 = int(self.n[1])
+        grid, out = np.zeros(n1), np.zeros(n1)
+        cf = None if ct is None else _state(ct)
+        _check(lib().mpc_pes_summed(self._h, int(electrons), float(threshold), _ptr(cf),
+                                    _ptr(grid), _ptr(out), n1))
+        return grid, out
 
     # -- objective and adjoint gradient -------------------------------------
     def objective_threshold(self, thr):

@@ -291,6 +291,58 @@ class Reference:
         return xf.view(np.complex128)
 
 
+class ReferencePes:
+    """The reference's own src/pes/pes.cpp (genPES1e / genPES2e), built by
+    oracle/Makefile against in-memory stand-ins for its HDF5 and yaml
+    libraries."""
+
+    PATH = os.path.join(HERE, "_ref", "libref_pes.so")
+
+    def __init__(self, path=None):
+        self.lib = _load(path or self.PATH)
+        self.lib.ref_pes.argtypes = [C.c_int, C.c_int, C.c_int, _ip, _ip, _dp, C.c_double, _dp,
+                                     C.c_char_p, C.c_char_p, C.c_size_t]
+
+    @classmethod
+    def available(cls):
+        return os.path.exists(cls.PATH)
+
+    def run(self, electrons, n, file_eig, ct, e0_1e=0.0, summed=True):
+        """Runs genPES1e / genPES2e on `ct` with the block energies
+        `file_eig` (a list of per-block arrays, each at least n[L] long: the
+        files' full contents).  Returns {"blocks": [rows of each
+        <prefix>_pes<L>.dat], "summed": rows of <prefix>_pes.dat (or None),
+        "printed": {name: value}} -- the reference's own outputs."""
+        import tempfile
+
+        n = np.ascontiguousarray(n, dtype=np.int32)
+        fsz = np.array([len(e) for e in file_eig], dtype=np.int32)
+        fe = np.ascontiguousarray(np.concatenate(file_eig), dtype=np.float64)
+        cf = _as_f64(ct).copy()
+        buf = C.create_string_buffer(4096)
+        with tempfile.TemporaryDirectory() as d:
+            prefix = os.path.join(d, "out")
+            rc = self.lib.ref_pes(int(electrons), int(bool(summed)), len(n) - 1, _i(n), _i(fsz),
+                                  _d(fe), float(e0_1e), _d(cf), prefix.encode(), buf, 4096)
+            text = buf.value.decode()
+            if rc:
+                raise ValueError(f"ref_pes: {text}")
+
+            def rows(path):
+                if not os.path.exists(path) or os.path.getsize(path) == 0:
+                    return np.zeros((0, 2))
+                return np.loadtxt(path, ndmin=2)
+
+            blocks = [rows(f"{prefix}_pes{L}.dat") for L in range(len(n))]
+            summed_rows = rows(f"{prefix}_pes.dat") if summed else None
+        printed = {}
+        for line in text.splitlines():
+            if ":" in line:
+                k, v = line.split(":", 1)
+                printed[k.strip()] = float(v)
+        return {"blocks": blocks, "summed": summed_rows, "printed": printed}
+
+
 def pes_reference(n, eig, ct, electrons=1, threshold=0.0):
     """pes::genPES1e / genPES2e (src/pes/pes.cpp:48-262) restated with the
     same loops and first-match bins, on full-precision coefficients.
@@ -325,3 +377,37 @@ def pes_reference(n, eig, ct, electrons=1, threshold=0.0):
                 if o + i > 0:
                     exc += c2[o + i]
     return pes, c2[0], c2.sum(), ion_yield, exc
+
+
+def pes_summed_reference(n, eig, ct, electrons=1, threshold=0.0):
+    """The summed spectrum of `pes -s` restated: genPES1e adds the blocks'
+    binned spectra per bin (src/pes/pes.cpp:127-137); genPES2e bins every
+    state i >= 1 of every block onto the L = 1 energies, first matching bin
+    k in 1 .. n_1 - 1, whose upper neighbour for k = n_1 - 1 is the first
+    energy of L = 2 as the reference indexes its concatenated energies
+    (src/pes/pes.cpp:215-245).  Returns (grid [n_1], pes [n_1]): grid holds
+    E1[k] (1e) or E1[k] - threshold (2e); the reference writes the rows
+    0 <= k <= n_1 - 2 (1e: n_0 - 2) whose grid energy is positive."""
+    n = [int(v) for v in n]
+    offs = np.concatenate([[0], np.cumsum(n)])
+    c2 = np.abs(np.asarray(ct)) ** 2
+    E1 = np.asarray(eig[offs[1]:offs[2]], dtype=np.float64)
+    n1 = n[1]
+    out = np.zeros(n1)
+    if electrons == 1:
+        per_l, _, _, _, _ = pes_reference(n, eig, ct, 1)
+        for l in range(len(n)):
+            for k in range(1, n[0] - 1):
+                out[k] += per_l[l, k]
+        return E1.copy(), out
+    kmax = n1 - 1 if len(n) > 2 else n1 - 2
+    for L in range(len(n)):
+        for i in range(1, n[L]):
+            e = eig[offs[L] + i]
+            for k in range(1, kmax + 1):
+                nd = abs(E1[k] - E1[k - 1])
+                pd = abs(eig[offs[1] + k + 1] - E1[k])
+                if E1[k] - 0.5 * nd < e < E1[k] + 0.5 * pd:
+                    out[k] += c2[offs[L] + i] * 2.0 / (nd + pd)
+                    break
+    return E1 - threshold, out

@@ -7,7 +7,9 @@ Run in a checkout where the reference source tree is present:
 Every number here comes from oracle/_ref/libref_tdse.so, i.e. the
 reference's src/tdse/tdse.cpp (MatVecV / MatVecL, tdse::propV / propL) and
 src/tdse/pulse.cpp compiled as they are, with only the missing third-party
-pieces stood in (odeint's RKF78 step, a CBLAS).  Inputs are small seeded
+pieces stood in (odeint's RKF78 step, a CBLAS), or (pes.npz) from
+oracle/_ref/libref_pes.so, the reference's src/pes/pes.cpp compiled as it is
+against in-memory stand-ins for its HDF5 and yaml libraries.  Inputs are small seeded
 synthetic systems in the reference's layout, and (--long) the benchmark's
 1e hydrogen system from the structure restatement:
   cfg0_h1e.npz   one whole 10-cycle 800 nm 1e14 W/cm^2 pulse (11,032 steps,
@@ -86,6 +88,46 @@ def main():
         out[key + "_ctfiles"] = np.array(names)
         out[key + "_n"], out[key + "_eig"], out[key + "_dip"] = s.n, s.eig, s.dip
     np.savez_compressed(os.path.join(HERE, "propagate.npz"), **out)
+
+    # 4) photoelectron spectra: the reference's own pes::genPES1e / genPES2e
+    #    (src/pes/pes.cpp) with -s, on seeded coefficients
+    from oracle import ReferencePes
+
+    rp = ReferencePes()
+    out = {}
+    rng = np.random.default_rng(21)
+    s = hydrogen_like_1e(40, 3, gauge="l", seed=5)
+    files = [np.concatenate([s.eig[s.offs[L]:s.offs[L + 1]],
+                             s.eig[s.offs[L + 1] - 1] + np.arange(1, 5)]) for L in range(4)]
+    ct = rng.standard_normal(s.ntot) + 1j * rng.standard_normal(s.ntot)
+    ct /= np.linalg.norm(ct)
+    r = rp.run(1, s.n, files, ct)
+    out["e1_n"], out["e1_eig"], out["e1_ct"] = s.n, s.eig, ct
+    for L, rows in enumerate(r["blocks"]):
+        out[f"e1_block{L}"] = rows
+    out["e1_summed"] = r["summed"]
+    out["e1_printed"] = np.array([r["printed"]["ground state pop"], r["printed"]["norm"],
+                                  r["printed"]["yield"]])
+    # 2e: CI-like sorted energies per block, the He+ 1s threshold at -2
+    n2 = [30, 40, 45, 50]
+    eig2, files2 = [], []
+    for L, nL in enumerate(n2):
+        e = np.sort(rng.uniform(-2.9 + 0.3 * L, 3.0, nL + 3))
+        files2.append(e)
+        eig2.append(e[:nL])
+    eig2 = np.concatenate(eig2)
+    ct2 = rng.standard_normal(sum(n2)) + 1j * rng.standard_normal(sum(n2))
+    ct2[0] *= 8.0
+    ct2 /= np.linalg.norm(ct2)
+    r = rp.run(2, n2, files2, ct2, e0_1e=-2.0)
+    out["e2_n"], out["e2_eig"], out["e2_ct"] = np.array(n2), eig2, ct2
+    out["e2_threshold"] = np.array(-2.0)
+    for L, rows in enumerate(r["blocks"]):
+        out[f"e2_block{L}"] = rows
+    out["e2_summed"] = r["summed"]
+    out["e2_printed"] = np.array([r["printed"]["ground state pop"], r["printed"]["norm"],
+                                  r["printed"]["yield"], r["printed"]["excited population"]])
+    np.savez_compressed(os.path.join(HERE, "pes.npz"), **out)
     print("golden fixtures written to", HERE)
 
 

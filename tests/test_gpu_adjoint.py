@@ -150,6 +150,28 @@ def test_resident_and_streamed_adjoints_agree():
     assert np.max(np.abs(f1 - f2)) <= 1e-12 * np.max(np.abs(f2))
 
 
+@pytest.mark.parametrize("g", ["l", "v"])
+@pytest.mark.parametrize("steps,ckpt", [(301, 64), (128, 64), (50, 64), (37, 1)])
+def test_fused_reverse_pass_equals_per_segment_passes(g, steps, ckpt, monkeypatch):
+    """The fused reverse pass (each segment's recompute concurrent with the
+    next segment's sweep, one persistent launch) against the per-segment
+    resident launches (recompute, then sweep): the same arithmetic per row
+    and the same reduction orders, so the same gradient; segment counts from
+    1 to many, a short last segment, one-step segments."""
+    s, p, u, T, x0, _ = _problem(g, seed=9, steps=steps)
+    out = []
+    for fused in (True, False):
+        if not fused:
+            monkeypatch.setenv("MPC_NO_FUSED_ADJOINT", "1")
+        with mpc_tdse.Context.from_system(s) as ctx:
+            assert ctx.path == "resident"
+            out.append(ctx.objective_gradient(p, u, T, 0.0, 0.1, steps, x0, -1, ckpt))
+    (J1, g1, f1), (J2, g2, f2) = out
+    assert J1 == J2
+    assert np.max(np.abs(g1 - g2)) <= 1e-13 * np.max(np.abs(g2))
+    assert np.max(np.abs(f1 - f2)) <= 1e-13 * np.max(np.abs(f2))
+
+
 def test_mpc_adjoint_is_the_objective_gradient():
     """mpc_adjoint (one call from controls to gradient) returns exactly what
     mpc_objective_gradient returns."""

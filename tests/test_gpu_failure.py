@@ -63,6 +63,14 @@ def test_adjoint_forward_barrier_timeout_is_reported():
             ctx.objective(p, u, T, 0.0, 0.1, 40, x0, -1, 16)
         assert ei.value.code == -3
         ctx.set_wait_limit(2.0)
+        # the reverse pass's persistent launch
+        ctx.objective(p, u, T, 0.0, 0.1, 40, x0, -1, 16)
+        ctx.set_wait_limit(1e-3)
+        ctx.inject_barrier_timeout()
+        with pytest.raises(mpc_tdse.MpcError) as ei:
+            ctx.objective_backward()
+        assert ei.value.code == -3
+        ctx.set_wait_limit(2.0)
         J1, g1, _ = ctx.objective_gradient(p, u, T, 0.0, 0.1, 40, x0, -1, 16)
     assert J1 == J0
     assert np.array_equal(g1, g0)
