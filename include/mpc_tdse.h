@@ -280,6 +280,10 @@ int mpc_batch_objective(mpc_ctx *ctx, int B, const mpc_pulse *pulses, int K, con
                         const double *T, double t0, double dt, int steps, int target,
                         int ckpt_every, const double *ct0, double *J);
 int mpc_batch_objective_backward(mpc_ctx *ctx, double *grad_u, double *dJdF);
+/* The checkpoint interval and segment count the last mpc_batch_objective
+ * used (chosen there when its ckpt_every was <= 0) and the device bytes of its
+ * buffers; any output may be NULL. */
+int mpc_batch_objective_info(mpc_ctx *ctx, int *ckpt_every, int *segments, double *device_bytes);
 int mpc_batch_objective_gradient(mpc_ctx *ctx, int B, const mpc_pulse *pulses, int K,
                                  const double *u, const double *T, double t0, double dt,
                                  int steps, int target, int ckpt_every, const double *ct0,

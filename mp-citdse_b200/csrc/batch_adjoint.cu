@@ -453,6 +453,16 @@ int mpc_batch_objective(mpc_ctx* c, int B, const mpc_pulse* pulses, int K, const
   return MPC_OK;
 }
 
+int mpc_batch_objective_info(mpc_ctx* c, int* ckpt_every, int* segments, double* device_bytes) {
+  if (!c || !c->badj || !c->badj->have_forward)
+    return mpc_fail(MPC_ERR_ARG, "mpc_batch_objective_info needs a preceding mpc_batch_objective");
+  const mpc_badj_state* a = c->badj;
+  if (ckpt_every) *ckpt_every = a->ckpt;
+  if (segments) *segments = a->nseg;
+  if (device_bytes) *device_bytes = (double)badj_bytes(c, a->B, a->steps, a->ckpt);
+  return MPC_OK;
+}
+
 int mpc_batch_objective_backward(mpc_ctx* c, double* grad_u, double* dJdF) {
   if (!c || !c->badj || !c->badj->have_forward)
     return mpc_fail(MPC_ERR_ARG, "mpc_batch_objective_backward needs a preceding "

@@ -98,6 +98,7 @@ def lib():
                                       C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp,
                                       _dp]
     L.mpc_batch_objective_backward.argtypes = [C.c_void_p, _dp, _dp]
+    L.mpc_batch_objective_info.argtypes = [C.c_void_p, _ip, _ip, _dp]
     L.mpc_batch_autotune.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]
     L.mpc_batch_propagate.argtypes = [C.c_void_p, C.c_int, C.POINTER(Pulse), _dp, _dp, C.c_double,
                                       C.c_double, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
@@ -406,6 +407,12 @@ class Context:
                                          _ptr(J)))
         self._badj = (B, K, int(steps))
         return J
+
+    def batch_objective_info(self):
+        """{ckpt_every, segments, device_bytes} of the last batch_objective."""
+        k, n, b = C.c_int(), C.c_int(), C.c_double()
+        _check(lib().mpc_batch_objective_info(self._h, C.byref(k), C.byref(n), C.byref(b)))
+        return {"ckpt_every": k.value, "segments": n.value, "device_bytes": b.value}
 
     def batch_objective_backward(self):
         """(dJ/du [B, K], dJ/dF_n [B, steps]) of the last batch_objective."""

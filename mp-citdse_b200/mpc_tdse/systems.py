@@ -52,6 +52,53 @@ class System:
     def offs(self):
         return np.concatenate([[0], np.cumsum(self.n)]).astype(np.int64)
 
+    def coupling_norm(self, iters=60, device=None, seed=0):
+        """||C||_2 of the dipole coupling C (the symmetric block-tridiagonal
+        matrix of the length gauge; the velocity gauge's antisymmetric one has
+        the same singular values up to the signs of its blocks, so the same
+        power iteration on C^T C bounds both), by power iteration; device: a
+        torch device for large systems, or None (numpy).  With max|E| it
+        bounds the generator's spectral radius, max|E| + |F| ||C||_2, the
+        quantity an explicit RK step must keep inside its stability
+        interval."""
+        offs = self.offs
+        nb = len(self.n) - 1
+        if device is not None:
+            import torch
+
+            blocks = [torch.as_tensor(self.block(L), device=device) for L in range(nb)]
+            x = torch.as_tensor(np.random.default_rng(seed).standard_normal(self.ntot),
+                                device=device)
+            cat = torch.cat
+            norm = torch.linalg.norm
+        else:
+            blocks = [self.block(L) for L in range(nb)]
+            x = np.random.default_rng(seed).standard_normal(self.ntot)
+            cat = np.concatenate
+            norm = np.linalg.norm
+
+        def apply(v, s_lo, s_up):
+            # block L of the result: s_lo D_{L-1}^T v_{L-1} + s_up D_L v_{L+1}
+            parts = []
+            for L in range(nb + 1):
+                acc = 0.0
+                if L > 0:
+                    acc = acc + s_lo * (blocks[L - 1].T @ v[offs[L - 1]:offs[L]])
+                if L < nb:
+                    acc = acc + s_up * (blocks[L] @ v[offs[L + 1]:offs[L + 2]])
+                parts.append(acc)
+            return cat(parts)
+
+        # C: (1, s); C^T: (s, 1), s = +1 (length) or -1 (velocity)
+        s = 1.0 if self.gauge == "l" else -1.0
+        lam = 0.0
+        for _ in range(iters):
+            x = x / norm(x)
+            y = apply(apply(x, 1.0, s), s, 1.0)   # C^T C x
+            lam = float(norm(y))
+            x = y
+        return float(np.sqrt(lam))
+
     def block(self, L):
         """Dipole block L as a [n_L, n_{L+1}] view."""
         o = int((self.n[:L].astype(np.int64) * self.n[1:L + 1]).sum())

@@ -45,3 +45,19 @@ def test_thomas_reiche_kuhn_sum_rule():
     assert abs((2 * dE * Dl ** 2).sum() - 1.0) < 1e-10
     assert abs((2 * Dv ** 2 / dE).sum() - 1.0) < 1e-10
     assert abs((2 * Dl * Dv).sum() - 1.0) < 1e-10
+
+
+def test_coupling_norm_is_the_dense_spectral_norm():
+    """System.coupling_norm (power iteration on the blocks) against the
+    dense 2-norm of the assembled coupling, both gauges."""
+    from mpc_tdse.systems import random_system
+
+    for g in "lv":
+        s = random_system([30, 40, 25, 35], gauge=g, seed=1)
+        off = s.offs
+        C = np.zeros((s.ntot, s.ntot))
+        for L in range(len(s.n) - 1):
+            D = s.block(L)
+            C[off[L]:off[L + 1], off[L + 1]:off[L + 2]] = D if g == "l" else -D
+            C[off[L + 1]:off[L + 2], off[L]:off[L + 1]] = D.T
+        assert abs(s.coupling_norm(iters=300) - np.linalg.norm(C, 2)) < 1e-9
