@@ -111,17 +111,23 @@ struct StageArgs {
 
 // One BK-deep chunk of the tile product from shared memory into acc: the A
 // operand is D_{L-1}^T (IS_P, stored k-major) or sign * D_L (stored m-major).
+// Only the chunk's first nks 8-deep k-steps hold coupling (the rest of the
+// last chunk of a block is zero fill) and only this warp's first mt_lim
+// 16-row m-tiles hold rows of the block: the rest would add exact zeros or
+// rows that are never stored, so they are skipped (warp-uniform branches).
 template <int BN, bool IS_P>
 __device__ __forceinline__ void chunk_mma(const double* As, const double* Bs, int wm, int wn,
-                                          int gq, int tq, double sign,
+                                          int gq, int tq, double sign, int nks, int mt_lim,
                                           double (&acc)[Tile<BN>::WMT][Tile<BN>::WNT][4]) {
   constexpr int WMT = Tile<BN>::WMT, WNT = Tile<BN>::WNT;
   constexpr int LDB = BN + 4;
 #pragma unroll
   for (int ks = 0; ks < BK / 8; ++ks) {
+    if (ks >= nks) break;
     double af[WMT][4], bf[WNT][2];
 #pragma unroll
     for (int mt = 0; mt < WMT; ++mt) {
+      if (mt >= mt_lim) break;
       const int m = wm * (WMT * 16) + mt * 16 + gq;
       const int k = ks * 8 + tq;
       if constexpr (IS_P) {
@@ -144,9 +150,11 @@ __device__ __forceinline__ void chunk_mma(const double* As, const double* Bs, in
       bf[nt][1] = Bs[(k + 4) * LDB + n];
     }
 #pragma unroll
-    for (int mt = 0; mt < WMT; ++mt)
+    for (int mt = 0; mt < WMT; ++mt) {
+      if (mt >= mt_lim) break;
 #pragma unroll
       for (int nt = 0; nt < WNT; ++nt) dmma16x8x8(acc[mt][nt], af[mt], bf[nt]);
+    }
   }
 }
 
@@ -191,6 +199,9 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   const int nchP = (KP + BK - 1) / BK, nchQ = (KQ + BK - 1) / BK;
   const int nch = nchP + nchQ;
   const double qsign = (a.gauge == 1) ? -1.0 : 1.0;
+  // this warp's m-tiles that hold rows of block L
+  const int wrows = nL - r0 - wm * (Tile<BN>::WMT * 16);
+  const int mt_lim = wrows <= 0 ? 0 : min(Tile<BN>::WMT, (wrows + 15) / 16);
 
   pdl_wait();
   const double* Yin = reinterpret_cast<const double*>(a.Yin);
@@ -281,10 +292,14 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
     }
     const double* As = bsm + (ci % NSTB) * (A_STAGE + B_STAGE);
     const double* Bs = As + A_STAGE;
+    // valid k-steps of this chunk: the coupled block's columns left from k0
+    const int chg = ch0 + ci;
+    const int krem = (chg < nchP) ? KP - chg * BK : KQ - (chg - nchP) * BK;
+    const int nks = min(BK / 8, (krem + 7) / 8);
     if (ci < nPm)
-      chunk_mma<BN, true>(As, Bs, wm, wn, gq, tq, 1.0, accP);
+      chunk_mma<BN, true>(As, Bs, wm, wn, gq, tq, 1.0, nks, mt_lim, accP);
     else
-      chunk_mma<BN, false>(As, Bs, wm, wn, gq, tq, qsign, accQ);
+      chunk_mma<BN, false>(As, Bs, wm, wn, gq, tq, qsign, nks, mt_lim, accQ);
   }
   cp_wait<0>();
   if constexpr (SPLIT) {
