@@ -380,6 +380,22 @@ int launch_stage(mpc_ctx* c, const StageArgs& a) {
   return MPC_OK;
 }
 
+// Product p = 0 .. 11 of a fixed-step (frozen-field) step evaluated as the
+// stability polynomial by Horner's rule: v_12 = G[12] x, then
+// v_m = h M(F) v_{m+1} + G[m] x for m = 11 .. 0, and v_0 = x_new.  Product p
+// forms v_{11-p}; the same ping-pong buffers as the stage form, so x_new
+// lands in Y[0].
+int launch_horner(mpc_ctx* c, int p, int ncol) {
+  StageArgs a = stage_args(c, p, ncol, 1.0, 1.0, false);
+  a.hg = rkf78::G[11 - p];
+  a.vscale = (p == 0) ? rkf78::G[12] : 1.0;
+  a.hlast = (p == 11) ? 1 : 0;
+  ProfScope ps(c, MPC_KERNEL_BATCH_STAGE);
+  ++c->launches;
+  CK(launch_variant<2>(c->stream, mpc_batch_variant(c, a.ncol), a));
+  return MPC_OK;
+}
+
 // Times every variant on a single right-hand side (stage 0, k only) at
 // widths 1, 2, 4, ... up to max_cols pulses and keeps the fastest per width.
 // Every variant sums in the same order, so the choice affects speed only.
@@ -562,6 +578,7 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
   aa.ntot = n;
   aa.ldc = ldc;
   aa.fx = fx;
+  if (fx.on) aa.Xn = b->Y[0];  // the Horner products leave x_new in Y[0]
 
   int ncol = B;
   ca.ncol = ncol;
@@ -648,8 +665,13 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
   // One attempted step of every active pulse: 13 stage GEMMs, the step
   // controller, the accepted-state update and the retirement flags.
   auto launch_attempt = [&]() -> int {
-    for (int st = 0; st < kNumStages; ++st)
-      if ((rc = launch_stage(c, stage_args(c, st, ncol, rtol, atol, false)))) return rc;
+    if (fx.on) {  // frozen field: 12 products of the stability polynomial
+      for (int p = 0; p < 12; ++p)
+        if ((rc = launch_horner(c, p, ncol))) return rc;
+    } else {
+      for (int st = 0; st < kNumStages; ++st)
+        if ((rc = launch_stage(c, stage_args(c, st, ncol, rtol, atol, false)))) return rc;
+    }
     ca.ncol = ncol;
     aa.ncol = ncol;
     {
@@ -704,7 +726,7 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
     }
     if (use_graph) {
       CK(cudaGraphLaunch(gexec, c->stream));
-      c->launches += 16LL * check_every;
+      c->launches += (fx.on ? 15LL : 16LL) * check_every;
       return MPC_OK;
     }
     for (int k = 0; k < check_every; ++k)

@@ -96,6 +96,12 @@ struct StageArgs {
   int nrowtiles;
   int want_k_only;       // 1: stop after storing k_s (single RHS evaluations)
   int fs_stride;         // ldc (a field per stage) or 0 (one field per step)
+  // MODE 2 (a frozen-field step as its stability polynomial, by Horner's
+  // rule): Yout = h M(F) (vscale Yin) + hg X; the last product (hlast) also
+  // forms the per-pulse norm partials of x_new = Yout
+  double hg;
+  double vscale;
+  int hlast;
   // adjoint stages (MODE 1): Yin = kbar_s, K = ybar slabs, Yout = kbar_{s-1}
   // (or lambda_n after stage 0)
   const double2* Ys;     // the forward stage input y_s
@@ -346,6 +352,72 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
     for (int j = 0; j < WN_TILES; ++j)
 #pragma unroll
       for (int v = 0; v < 4; ++v) acc[i][j][v] = accP[i][j][v] + accQ[i][j][v];
+
+  if constexpr (MODE == 2) {
+    // ---------------- Horner epilogue (fixed step, frozen field) ----------------
+    __shared__ double red_h[BM / 16][BN / 2];
+#pragma unroll
+    for (int nt = 0; nt < WN_TILES; ++nt) {
+      const int q = (c0 + wn * (WNT * 8) + nt * 8) / 2 + tq;  // pulse column
+      const bool qv = q < a.ncol;
+      double nsum[WM_TILES];
+#pragma unroll
+      for (int mt = 0; mt < WM_TILES; ++mt) nsum[mt] = 0.0;
+      const double F = qv ? a.Fs[q] : 0.0;
+      const double hq = qv ? a.h[q] : 0.0;
+      const double vs = a.vscale, gm = a.hg;
+#pragma unroll
+      for (int mt = 0; mt < WM_TILES; ++mt)
+#pragma unroll
+        for (int hr = 0; hr < 2; ++hr) {
+          const int r = r0 + wm * (WMT * 16) + mt * 16 + gq + 8 * hr;
+          if (!qv || r >= nL) continue;
+          const long long i = g.state_off[L] + r;
+          const long long idx = i * a.ldc + q;
+          const double wre = vs * acc[mt][nt][2 * hr], wim = vs * acc[mt][nt][2 * hr + 1];
+          const double2 v0 = a.Yin[idx];
+          const double2 v = make_double2(vs * v0.x, vs * v0.y);
+          const double2 x = a.X[idx];
+          const double e = a.eps[i];
+          double kre, kim;  // M(F) v, formed as the stage form forms k
+          if (a.gauge == 0) {
+            kre = fma(F, wim, e * v.y);
+            kim = -fma(F, wre, e * v.x);
+          } else {
+            kre = fma(F, wre, e * v.y);
+            kim = fma(F, wim, -e * v.x);
+          }
+          const double2 o = make_double2(fma(hq, kre, gm * x.x), fma(hq, kim, gm * x.y));
+          a.Yout[idx] = o;
+          if (a.hlast) nsum[mt] += o.x * o.x + o.y * o.y;
+        }
+      if (a.hlast) {
+#pragma unroll
+        for (int o = 4; o < 32; o <<= 1)
+#pragma unroll
+          for (int mt = 0; mt < WM_TILES; ++mt)
+            nsum[mt] += __shfl_xor_sync(0xffffffffu, nsum[mt], o);
+        const int col = wn * (WNT * 4) + nt * 4 + tq;
+        if (gq == 0) {
+#pragma unroll
+          for (int mt = 0; mt < WM_TILES; ++mt) red_h[wm * WMT + mt][col] = nsum[mt];
+        }
+      }
+    }
+    if (a.hlast) {
+      __syncthreads();
+      if (threadIdx.x < BN / 2) {
+        const int q = c0 / 2 + threadIdx.x;
+        if (q < a.ncol) {
+          double ns = red_h[0][threadIdx.x];
+#pragma unroll
+          for (int m = 1; m < BM / 16; ++m) ns += red_h[m][threadIdx.x];
+          a.normpart[(long long)rtile * a.ldc + q] = ns;
+        }
+      }
+    }
+    return;
+  }
 
   if constexpr (MODE == 1) {
     // ---------------- adjoint epilogue ----------------
@@ -654,6 +726,7 @@ inline int stage_setup(int device) {
   CK(cudaMemcpyToSymbol(c_C, Cn, sizeof Cn));
   CK(set_stage_attrs<0>());
   CK(set_stage_attrs<1>());
+  CK(set_stage_attrs<2>());
   done[device] = true;
   return MPC_OK;
 }

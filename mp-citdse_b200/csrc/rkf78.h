@@ -35,6 +35,26 @@ constexpr double B8[13] = {0, 0, 0, 0, 0, F_(34, 105), F_(9, 35), F_(9, 35), F_(
 // 7th-order weights: used only through the embedded error estimate.
 constexpr double B7[13] = {F_(41, 840), 0, 0, 0, 0, F_(34, 105), F_(9, 35), F_(9, 35),
                            F_(9, 280), F_(9, 280), F_(41, 840), 0, 0};
+// Coefficients of the 8th-order solution's stability polynomial
+// R(z) = 1 + z b8^T (I - zA)^{-1} 1 = sum_m G[m] z^m: G[m] = b8^T A^(m-1) 1
+// for m >= 1, evaluated in exact rational arithmetic from the fractions
+// above.  G[m] = 1/m! up to m = 8 (the method's order); the z^13 coefficient
+// vanishes (a_{11,10} = 0 breaks the only chain through all 13 stages), so
+// R has degree 12.  With the field frozen over a step the system is linear
+// and autonomous, and one step is x_new = R(hM) x exactly (up to rounding).
+constexpr double G[13] = {1,
+                          1,
+                          F_(1, 2),
+                          F_(1, 6),
+                          F_(1, 24),
+                          F_(1, 120),
+                          F_(1, 720),
+                          F_(1, 5040),
+                          F_(1, 40320),
+                          F_(491, 209018880),
+                          F_(1333, 5643509760LL),
+                          F_(-13, 501645312),
+                          F_(-65, 4514807808LL)};
 #undef F_
 
 }  // namespace rkf78

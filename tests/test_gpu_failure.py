@@ -77,7 +77,9 @@ def test_adjoint_forward_barrier_timeout_is_reported():
 
 
 def test_batched_resident_tail_barrier_timeout_is_reported():
-    h = hydrogen_like_1e(24, 2, gauge="l", seed=4)
+    # 3 blocks of 80 states: every one of the 148 CTAs of the resident batched
+    # kernel gets rows (a much smaller system does not take that path)
+    h = hydrogen_like_1e(80, 2, gauge="l", seed=4)
     x = np.zeros(h.ntot, complex)
     x[0] = 1.0
     T = 5.0

@@ -9,6 +9,7 @@ import math
 import os
 import tempfile
 
+
 import numpy as np
 import pytest
 import scipy.linalg
@@ -230,3 +231,36 @@ def test_pes_restatement_known_answers():
     assert pes2[0, 5] == 0.0                                 # the top state has no upper edge
     assert abs(y2 - (0.04 + 0.09 + 0.01)) < 1e-15
     assert abs(exc2 - (0.01 + 0.04 + 0.09 + 0.01)) < 1e-15
+
+
+def test_frozen_field_step_is_the_degree_12_stability_polynomial(oracle):
+    """With F frozen over a step the system is linear and autonomous, so one
+    RKF78 step (8th-order solution) is R(hM) x with R(z) = sum_m G_m z^m,
+    G_m = b8^T A^(m-1) 1: degree 12 (the z^13 coefficient vanishes).  The
+    batched fixed-step path evaluates the step this way, by Horner's rule
+    (12 products with M instead of 13 stage slopes); here the identity is
+    checked against the stage form of the restatement."""
+    from mpc_tdse.systems import random_system
+
+    A, b8, _, _ = oracle.tableau()
+    G = [1.0]
+    v = np.ones(13)
+    for _ in range(13):
+        G.append(float(b8 @ v))
+        v = A @ v
+    assert G[13] == 0.0
+    assert all(abs(G[m] - 1.0 / math.factorial(m)) <= 1e-14 * G[m] for m in range(9))
+    for g in "lv":
+        s = random_system([20, 25, 18], gauge=g, seed=2, e_max=6.0)
+        rng = np.random.default_rng(3)
+        x = rng.standard_normal(s.ntot) + 1j * rng.standard_normal(s.ntot)
+        F, h = 0.31, 0.07
+        want = oracle.rk78_step(s.n, s.eig, s.dip, g, F, h, x)
+
+        def M(y):
+            return oracle.rhs(s.n, s.eig, s.dip, g, F, y)
+
+        hv = G[12] * x
+        for m in range(11, -1, -1):
+            hv = h * M(hv) + G[m] * x
+        assert np.max(np.abs(hv - want)) < 1e-13
