@@ -19,6 +19,8 @@ TDSE = os.path.join(PKG, "bin", "tdse")
 # the system C++ compiler (an environment CXX may link libstdc++ statically,
 # which breaks iostreams inside a library loaded by Python)
 CXX = "g++"
+# NVTX (header-only) for the executable's profiler ranges
+CUDA_INCLUDE = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
          "-Xptxas", "-v", "--expt-relaxed-constexpr"]
@@ -63,7 +65,8 @@ def build_host(force=False, verbose=False):
         jobs.append([CXX, "-std=c++17", "-O2", "-o", TDSE,
                      os.path.join(PKG, "host", "tdse_main.cpp"),
                      os.path.join(PKG, "host", "h5lite.cpp"),
-                     "-I", os.path.join(ROOT, "include"), "-L", os.path.dirname(LIB), "-lmpc_tdse",
+                     "-I", os.path.join(ROOT, "include"), "-I", CUDA_INCLUDE,
+                     "-L", os.path.dirname(LIB), "-lmpc_tdse",
                      "-Wl,-rpath,$ORIGIN/../lib"])
     for cmd in jobs:
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -382,6 +382,7 @@ extern "C" {
 int mpc_objective(mpc_ctx* c, const mpc_pulse* p, int K, const double* u, double T, double t0,
                   double dt, int steps, int target, int ckpt_every, const double* ct0,
                   double* J) {
+  NvtxRange nvtx_("mpc_objective (forward)");
   if (!c || !p || !ct0 || !J || steps <= 0 || !(dt > 0.0) || (K > 0 && !u) || K == 1)
     return mpc_fail(MPC_ERR_ARG, "bad argument");
   if (target >= c->g.ntot) return mpc_fail(MPC_ERR_ARG, "target out of range");
@@ -472,6 +473,7 @@ int mpc_objective_threshold(mpc_ctx* c, double thr) {
 }
 
 int mpc_objective_backward(mpc_ctx* c, double* grad_u, double* dJdF) {
+  NvtxRange nvtx_("mpc_objective_backward");
   if (!c || !c->adj || !c->adj->have_forward)
     return mpc_fail(MPC_ERR_ARG, "mpc_objective_backward needs a preceding mpc_objective");
   CK(cudaSetDevice(c->device));

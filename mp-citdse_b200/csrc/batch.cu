@@ -805,6 +805,7 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
                         const double* t_end, double h0, double dt_max, double rtol, double atol,
                         int max_attempts, double* ct, int* accepted, int* rejected,
                         double* t_final) {
+  NvtxRange nvtx_("mpc_batch_propagate");
   if (!c || !pulses || !t0 || !t_end || !ct || B <= 0)
     return mpc_fail(MPC_ERR_ARG, "bad argument");
   if (!(h0 > 0.0) || !(dt_max > 0.0) || !(rtol >= 0.0) || !(atol >= 0.0) || rtol + atol <= 0.0)
@@ -821,6 +822,7 @@ int mpc_batch_propagate(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
 int mpc_batch_advance(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, double dt,
                       const int* steps, int pop_index, double* ct, double* pop_out,
                       double* norm_out) {
+  NvtxRange nvtx_("mpc_batch_advance");
   if (!c || !pulses || !t0 || !steps || !ct || B <= 0)
     return mpc_fail(MPC_ERR_ARG, "bad argument");
   if (!(dt > 0.0)) return mpc_fail(MPC_ERR_ARG, "dt must be > 0");

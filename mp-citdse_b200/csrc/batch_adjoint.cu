@@ -352,6 +352,7 @@ extern "C" {
 int mpc_batch_objective(mpc_ctx* c, int B, const mpc_pulse* pulses, int K, const double* u,
                         const double* T, double t0, double dt, int steps, int target,
                         int ckpt_every, const double* ct0, double* J) {
+  NvtxRange nvtx_("mpc_batch_objective (forward)");
   if (!c || !pulses || !ct0 || !J || B <= 0 || steps <= 0 || !(dt > 0.0) || K == 1 ||
       (K > 0 && (!u || !T)))
     return mpc_fail(MPC_ERR_ARG, "bad argument");
@@ -464,6 +465,7 @@ int mpc_batch_objective_info(mpc_ctx* c, int* ckpt_every, int* segments, double*
 }
 
 int mpc_batch_objective_backward(mpc_ctx* c, double* grad_u, double* dJdF) {
+  NvtxRange nvtx_("mpc_batch_objective_backward");
   if (!c || !c->badj || !c->badj->have_forward)
     return mpc_fail(MPC_ERR_ARG, "mpc_batch_objective_backward needs a preceding "
                                  "mpc_batch_objective");

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <string>
 #include <utility>
@@ -104,6 +105,15 @@ cudaError_t mpc_launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t
   cfg.numAttrs = mpc_pdl_enabled() ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kern, args...);
 }
+
+// An NVTX range for the duration of a scope (a named region on a profiler's
+// timeline; no cost without a profiler attached).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Event bracket for profiling one launch of kernel kind `kind`.
 struct ProfScope {

@@ -469,6 +469,7 @@ double mpc_field(const mpc_pulse* p, double t) { return p ? host_field(*p, t) : 
 
 int mpc_ctx_create(int L_max, const int* state_sz, const double* eig, const double* dip,
                    char gauge, int device, mpc_ctx** out) {
+  NvtxRange nvtx_("mpc_ctx_create (upload)");
   if (!out) return fail(MPC_ERR_ARG, "null output");
   *out = nullptr;
   if (L_max < 1 || L_max >= kMaxBlocks)
@@ -673,6 +674,7 @@ int mpc_state_get(mpc_ctx* c, double* ct) {
 
 int mpc_advance(mpc_ctx* c, const mpc_pulse* p, double t0, double dt, int steps,
                 int pop_index) {
+  NvtxRange nvtx_("mpc_advance");
   if (!c || !p) return fail(MPC_ERR_ARG, "null argument");
   if (steps < 0) return fail(MPC_ERR_ARG, "steps < 0");
   if (pop_index < 0 || pop_index >= c->g.ntot) return fail(MPC_ERR_ARG, "pop_index out of range");
@@ -705,6 +707,7 @@ int mpc_history_get(mpc_ctx* c, int steps, double* pop_out, double* field_out,
 int mpc_propagate(mpc_ctx* c, const mpc_pulse* p, double t0, double dt, int steps,
                   int pop_index, double* ct, double* pop_out, double* field_out,
                   double* norm_out) {
+  NvtxRange nvtx_("mpc_propagate");
   if (!c || !p || !ct) return fail(MPC_ERR_ARG, "null argument");
   int rc;
   if ((rc = mpc_state_set(c, ct))) return rc;

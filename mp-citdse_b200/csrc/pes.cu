@@ -222,6 +222,7 @@ extern "C" int mpc_pes_summed(mpc_ctx* c, int electrons, double threshold, const
 
 extern "C" int mpc_pes(mpc_ctx* c, int electrons, double threshold, const double* ct, double* pes,
                        int ngrid, double* stats) {
+  NvtxRange nvtx_("mpc_pes");
   if (!c || !pes || !stats || (electrons != 1 && electrons != 2))
     return mpc_fail(MPC_ERR_ARG, "bad argument");
   const Geometry& g = c->g;

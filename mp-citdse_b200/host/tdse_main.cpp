@@ -28,11 +28,24 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/mpc_tdse.h"
 #include "h5lite.hpp"
 #include "yaml_lite.hpp"
 
 namespace {
+
+// A named region on a profiler's timeline (load / propagate / output).
+struct Range {
+  bool open = true;
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  void end() {
+    if (open) nvtxRangePop();
+    open = false;
+  }
+  ~Range() { end(); }
+};
 
 constexpr double kEvAu = 1. / 27.211396181;  // conv::En_ev_au_ (src/include/au.hpp:30-31)
 
@@ -219,6 +232,7 @@ int run(int argc, char* argv[]) {
   // tdrd::readEnergies / readDipoles: the top-left state_sz blocks
   std::vector<int> offs{0};
   std::vector<double> eig, dip;
+  Range load_range("tdse: load inputs");
   for (int L = 0; L <= cf.L_max; ++L) {
     const auto e = h5::read_block(en_pot + std::to_string(L) + ".h5", en_set, cf.state_sz[L], 0);
     eig.insert(eig.end(), e.begin(), e.end());
@@ -249,6 +263,7 @@ int run(int argc, char* argv[]) {
     std::cout << "Start time (a.u.): " << t << "\n";
     read_init_ct(init_ct, ct_sz, ct);
   }
+  load_range.end();
   const double tau = mpc_period(cf.w * kEvAu, cf.cycles);
   const int steps = (tau - t) / cf.dt;
   double auIo, auw;
@@ -278,7 +293,11 @@ int run(int argc, char* argv[]) {
   int st = 0;
   while (st < steps) {
     const int n = (st == 0) ? 1 : std::min(print, steps - st);
-    check(mpc_advance(ctx, &pulse, t, cf.dt, n, pop_index));
+    {
+      Range r("tdse: propagate");
+      check(mpc_advance(ctx, &pulse, t, cf.dt, n, pop_index));
+    }
+    Range out_range("tdse: output");
     pop.resize(n + 1);
     fld.resize(n);
     check(mpc_history_get(ctx, n, pop.data(), fld.data(), nullptr));
