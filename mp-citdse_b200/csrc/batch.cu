@@ -281,6 +281,8 @@ struct mpc_batch_state {
   int* map = nullptr;
   double* ws = nullptr;     // split-variant workspace
   int* cnt = nullptr;       // split-variant arrival counters (kept at zero)
+  unsigned* hcnt = nullptr; // persistent Horner launch: ticket + per-column progress
+  size_t hcnt_n = 0;
   void* scratch = nullptr;  // compaction staging for per-column scalars
   ColState c{};
   PulseResults res{};
@@ -315,6 +317,7 @@ int ensure_batch(mpc_ctx* c, int B) {
   for (int L = 0; L < g.nstate_blk; ++L)
     nrt += (g.state_off[L + 1] - g.state_off[L] + BM - 1) / BM;
   b->nrowtiles = nrt;
+  b->hcnt_n = 1 + 12 * (size_t)((2 * ldc + 15) / 16) * kMaxBlocks;
   const size_t nel = (size_t)g.ntot * ldc;
   int rc;
   ColState& s = b->c;
@@ -325,6 +328,7 @@ int ensure_batch(mpc_ctx* c, int B) {
       (rc = balloc(b, &b->map, ldc)) ||
       (rc = balloc(b, &b->ws, split_ws_doubles(nrt, ldc))) ||
       (rc = balloc(b, &b->cnt, split_cnt_ints(nrt, ldc))) ||
+      (rc = balloc(b, &b->hcnt, 1 + 12 * (size_t)((2 * ldc + 15) / 16) * kMaxBlocks)) ||
       (rc = balloc(b, reinterpret_cast<char**>(&b->scratch), sizeof(mpc_pulse) * ldc)) ||
       (rc = balloc(b, &s.pulse, ldc)) || (rc = balloc(b, &s.t, ldc)) ||
       (rc = balloc(b, &s.t_end, ldc)) || (rc = balloc(b, &s.h, ldc)) ||
@@ -377,6 +381,41 @@ int launch_stage(mpc_ctx* c, const StageArgs& a) {
   ProfScope ps(c, MPC_KERNEL_BATCH_STAGE);
   ++c->launches;
   CK(launch_variant<0>(c->stream, mpc_batch_variant(c, a.ncol), a));
+  return MPC_OK;
+}
+
+// The 12 Horner products of a fixed step in one persistent launch
+// (k_batch_horner), when a product has enough tiles to fill the GPU; the
+// tile shape is the tuned variant's for this width.
+bool horner_persistent(mpc_ctx* c, int ncol) {
+  static const bool off = std::getenv("MPC_NO_PERSIST") != nullptr;
+  if (off) return false;
+  const int bn = horner_tile_bn(mpc_batch_variant(c, ncol));
+  const int ncolt = (2 * ncol + bn - 1) / bn;
+  return (long long)ncolt * c->batch->nrowtiles >= c->num_sms;
+}
+
+int launch_horner_persistent(mpc_ctx* c, int ncol) {
+  mpc_batch_state* b = c->batch;
+  const int v = mpc_batch_variant(c, ncol);
+  const int bn = horner_tile_bn(v);
+  HornerArgs h{};
+  h.a = stage_args(c, 0, ncol, 1.0, 1.0, false);
+  h.Y[0] = b->Y[0];
+  h.Y[1] = b->Y[1];
+  h.ticket = b->hcnt;
+  h.done = b->hcnt + 1;
+  h.status = c->d_status;
+  const BarrierCfg bc = mpc_barrier_cfg(c);
+  h.wait_ns = bc.wait_ns;
+  h.skew = (unsigned)bc.skew;
+  h.ncolt = (2 * ncol + bn - 1) / bn;
+  const int items = 12 * h.ncolt * b->nrowtiles;
+  CK(cudaMemsetAsync(b->hcnt, 0, sizeof(unsigned) * (1 + 12 * (size_t)h.ncolt * c->g.nstate_blk),
+                     c->stream));
+  ProfScope ps(c, MPC_KERNEL_BATCH_STAGE);
+  ++c->launches;
+  CK(launch_horner_variant(c->stream, v, h, c->num_sms, items));
   return MPC_OK;
 }
 
@@ -665,7 +704,9 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
   // One attempted step of every active pulse: 13 stage GEMMs, the step
   // controller, the accepted-state update and the retirement flags.
   auto launch_attempt = [&]() -> int {
-    if (fx.on) {  // frozen field: 12 products of the stability polynomial
+    if (fx.on && horner_persistent(c, ncol)) {  // frozen field, one persistent launch
+      if ((rc = launch_horner_persistent(c, ncol))) return rc;
+    } else if (fx.on) {  // frozen field: 12 products of the stability polynomial
       for (int p = 0; p < 12; ++p)
         if ((rc = launch_horner(c, p, ncol))) return rc;
     } else {
@@ -726,7 +767,7 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
     }
     if (use_graph) {
       CK(cudaGraphLaunch(gexec, c->stream));
-      c->launches += (fx.on ? 15LL : 16LL) * check_every;
+      c->launches += (fx.on ? (horner_persistent(c, ncol) ? 4LL : 15LL) : 16LL) * check_every;
       return MPC_OK;
     }
     for (int k = 0; k < check_every; ++k)

@@ -16,6 +16,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "ctx.h"
 #include "dev_util.cuh"
 #include "plan.h"
@@ -164,16 +166,32 @@ __device__ __forceinline__ void chunk_mma(const double* As, const double* Bs, in
   }
 }
 
+// One output tile of a stage (or Horner product): tile index `bid` (the
+// block index of the one-launch-per-stage kernel below, or a work item of the
+// persistent kernel), shared-memory ring `bsm`.
+// The fields that change from one stage (or Horner product) to the next;
+// the rest of StageArgs is shared by all of a step's launches.
+struct ProdSel {
+  const double2* Yin;
+  double2* Yout;
+  int stage;
+  double hg, vscale;
+  int hlast;
+};
+
+__device__ __forceinline__ ProdSel prod_sel(const StageArgs& a) {
+  return ProdSel{a.Yin, a.Yout, a.stage, a.hg, a.vscale, a.hlast};
+}
+
 template <int BN, int NSTB, int MODE, int SPLIT>
-__global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_constant__ StageArgs a) {
-  extern __shared__ __align__(16) double bsm[];
+__device__ __forceinline__ void stage_tile(const StageArgs& a, const ProdSel& ps, const int bid,
+                                           double* bsm) {
   constexpr int WGM = Tile<BN>::WGM, WMT = Tile<BN>::WMT, WNT = Tile<BN>::WNT;
   constexpr int LDB = BN + 4;
   constexpr int B_STAGE = b_stage<BN>();
   constexpr int WM_TILES = WMT, WN_TILES = WNT;
   static_assert(Tile<BN>::WGM * Tile<BN>::WGN * 32 == BTHREADS, "8 warps");
   static_assert(WGM * WMT * 16 == BM && Tile<BN>::WGN * WNT * 8 == BN, "tile shape");
-  pdl_trigger();
   const Geometry& g = a.g;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gq = lane >> 2, tq = lane & 3;
@@ -183,8 +201,8 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   // k half varying fastest: CTAs that read the same coupling rows run side by
   // side and share them through L2.
   const int ncolt = (2 * a.ncol + BN - 1) / BN;
-  const int zk = SPLIT ? (int)(blockIdx.x & 1) : 0;
-  const int tp = SPLIT ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;  // tile pair
+  const int zk = SPLIT ? (bid & 1) : 0;
+  const int tp = SPLIT ? (bid >> 1) : bid;  // tile pair
   const int rtile = tp / ncolt;
   // row tile -> state block L and first local row r0
   int L = 0, rt = rtile;
@@ -210,7 +228,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   const int mt_lim = wrows <= 0 ? 0 : min(Tile<BN>::WMT, (wrows + 15) / 16);
 
   pdl_wait();
-  const double* Yin = reinterpret_cast<const double*>(a.Yin);
+  const double* Yin = reinterpret_cast<const double*>(ps.Yin);
 
   // Each thread's cp.async assignments are fixed for the whole K loop, so
   // their source pointers and bounds are set up once; a chunk only adds its
@@ -365,7 +383,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
       for (int mt = 0; mt < WM_TILES; ++mt) nsum[mt] = 0.0;
       const double F = qv ? a.Fs[q] : 0.0;
       const double hq = qv ? a.h[q] : 0.0;
-      const double vs = a.vscale, gm = a.hg;
+      const double vs = ps.vscale, gm = ps.hg;
 #pragma unroll
       for (int mt = 0; mt < WM_TILES; ++mt)
 #pragma unroll
@@ -375,7 +393,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
           const long long i = g.state_off[L] + r;
           const long long idx = i * a.ldc + q;
           const double wre = vs * acc[mt][nt][2 * hr], wim = vs * acc[mt][nt][2 * hr + 1];
-          const double2 v0 = a.Yin[idx];
+          const double2 v0 = ps.Yin[idx];
           const double2 v = make_double2(vs * v0.x, vs * v0.y);
           const double2 x = a.X[idx];
           const double e = a.eps[i];
@@ -388,10 +406,10 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
             kim = fma(F, wim, -e * v.x);
           }
           const double2 o = make_double2(fma(hq, kre, gm * x.x), fma(hq, kim, gm * x.y));
-          a.Yout[idx] = o;
-          if (a.hlast) nsum[mt] += o.x * o.x + o.y * o.y;
+          ps.Yout[idx] = o;
+          if (ps.hlast) nsum[mt] += o.x * o.x + o.y * o.y;
         }
-      if (a.hlast) {
+      if (ps.hlast) {
 #pragma unroll
         for (int o = 4; o < 32; o <<= 1)
 #pragma unroll
@@ -404,7 +422,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
         }
       }
     }
-    if (a.hlast) {
+    if (ps.hlast) {
       __syncthreads();
       if (threadIdx.x < BN / 2) {
         const int q = c0 / 2 + threadIdx.x;
@@ -421,7 +439,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
 
   if constexpr (MODE == 1) {
     // ---------------- adjoint epilogue ----------------
-    const int s = a.stage;
+    const int s = ps.stage;
     const long long nld = (long long)g.ntot * a.ldc;
     __shared__ double red_f[BM / 16][BN / 2];
 #pragma unroll
@@ -442,7 +460,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
           const long long i = g.state_off[L] + r;
           const long long idx = i * a.ldc + q;
           const double wre = acc[mt][nt][2 * hr], wim = acc[mt][nt][2 * hr + 1];
-          const double2 kb = a.Yin[idx];
+          const double2 kb = ps.Yin[idx];
           const double e = a.eps[i];
           // M(F) kbar (formed as the forward forms k) and M1 kbar = dM/dF kbar
           double gre, gim, mre, mim;
@@ -486,7 +504,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
               o.y += ybj.y;
             }
           }
-          a.Yout[idx] = o;
+          ps.Yout[idx] = o;
         }
 #pragma unroll
       for (int o = 4; o < 32; o <<= 1)
@@ -513,7 +531,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   }
 
   // ---------------- fused RK epilogue ----------------
-  const int s = a.stage;
+  const int s = ps.stage;
   const long long nld = (long long)g.ntot * a.ldc;  // complex elements per k slab
   const bool last = (s == kNumStages - 1);
   // norm partials per 16-row m-tile, summed over the tile's rows by a fixed
@@ -539,7 +557,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
         const long long i = g.state_off[L] + r;
         const long long idx = i * a.ldc + q;
         const double wre = acc[mt][nt][2 * hr], wim = acc[mt][nt][2 * hr + 1];
-        const double2 y = a.Yin[idx];
+        const double2 y = ps.Yin[idx];
         const double e = a.eps[i];
         double kre, kim;
         if (a.gauge == 0) {
@@ -586,7 +604,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
           if (!(ratio == ratio)) emax = ratio;  // keep a NaN
           nsum[mt] += o.x * o.x + o.y * o.y;
         }
-        a.Yout[idx] = o;
+        ps.Yout[idx] = o;
       }
     if (last && !a.want_k_only) {
       // per pulse and m-tile: this thread's two rows, then the 8 lanes
@@ -627,6 +645,109 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_consta
   }
 }
 
+
+template <int BN, int NSTB, int MODE, int SPLIT>
+__global__ void __launch_bounds__(BTHREADS, 2) k_batch_stage(const __grid_constant__ StageArgs a) {
+  extern __shared__ __align__(16) double bsm[];
+  pdl_trigger();
+  stage_tile<BN, NSTB, MODE, SPLIT>(a, prod_sel(a), (int)blockIdx.x, bsm);
+}
+
+// The 12 Horner products of one fixed step in one persistent launch.  Work
+// items are (product p, column tile c, row tile r), handed out in that order
+// by an atomic ticket; an item waits until product p-1 has finished every row
+// tile of the three blocks its rows couple to (L-1, L, L+1) in the same
+// column tile -- its GEMM operand rows and its own rows -- then runs the tile
+// exactly as the one-launch-per-product kernel would.  Pulse columns never
+// depend on each other, so the CTAs flow from one product into the next
+// without a grid-wide barrier: the last partial wave of one product overlaps
+// the first tiles of the next.  An item only waits for items with smaller
+// tickets, all of them already taken by running CTAs, so the launch needs no
+// co-residency guarantee.  Waits are bounded (the context's limit); one that
+// runs out raises the status word and ends the CTA, and the others then run
+// out of their own waits.  Item p's writes go to Y[(p+1)&1]; the rows it
+// overwrites were last read by product p-1 items that it waited for.
+struct HornerArgs {
+  StageArgs a;            // X, Y, D, fields, steps; the per-product fields are set here
+  const double2* Y[2];    // ping-pong of the products (Y[1] first)
+  unsigned* ticket;       // work counter, zero at launch
+  unsigned* done;         // [12][ncolt][nstate_blk] finished row tiles, zero at launch
+  unsigned* status;
+  unsigned long long wait_ns;
+  unsigned skew;          // 0; 1 when a test injects a dependency that cannot complete
+  int ncolt;              // column tiles
+};
+
+__constant__ double c_G[13];   // the stability polynomial's coefficients
+
+template <int BN, int NSTB>
+__global__ void __launch_bounds__(BTHREADS, 2) k_batch_horner(const __grid_constant__ HornerArgs h) {
+  extern __shared__ __align__(16) double bsm[];
+  __shared__ int s_item, s_dead;
+  const Geometry& g = h.a.g;
+  const int nrt = h.a.nrowtiles, ncolt = h.ncolt;
+  const int per = nrt * ncolt, total = 12 * per;
+  if (threadIdx.x == 0) s_dead = 0;
+  for (;;) {
+    __syncthreads();   // the previous tile's shared-memory reads are over
+    if (threadIdx.x == 0) {
+      s_item = (int)atomicAdd(h.ticket, 1u);
+      // another CTA's wait ran out: its items will never finish, stop now
+      if (*(volatile unsigned*)h.status & ST_WAIT_TIMEOUT) s_dead = 1;
+    }
+    __syncthreads();
+    const int item = s_item;
+    if (item >= total || s_dead) break;
+    const int p = item / per, w = item % per;
+    const int ct = w / nrt, rtile = w % nrt;   // column tile outer: products flow per column
+    int L = 0, rt = rtile;
+    while (true) {
+      const int nt = (g.state_off[L + 1] - g.state_off[L] + BM - 1) / BM;
+      if (rt < nt || L + 1 >= g.nstate_blk) break;
+      rt -= nt;
+      ++L;
+    }
+    if (p > 0 && threadIdx.x == 0) {
+      const unsigned* dn = h.done + ((size_t)(p - 1) * ncolt + ct) * g.nstate_blk;
+      const unsigned long long t0 = globaltimer_ns();
+      for (int Ld = max(L - 1, 0); Ld <= min(L + 1, g.nstate_blk - 1) && !s_dead; ++Ld) {
+        const unsigned need =
+            (unsigned)((g.state_off[Ld + 1] - g.state_off[Ld] + BM - 1) / BM) + h.skew;
+        for (unsigned it = 0;; ++it) {
+          unsigned v;
+          asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(dn + Ld) : "memory");
+          if (v >= need) break;
+          if ((it & 255u) == 255u) {
+            if (globaltimer_ns() - t0 > h.wait_ns) {
+              atomicOr(h.status, ST_WAIT_TIMEOUT);
+              s_dead = 1;
+              break;
+            }
+            if (*(volatile unsigned*)h.status & ST_WAIT_TIMEOUT) {  // another CTA gave up
+              s_dead = 1;
+              break;
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (s_dead) break;
+    ProdSel ps;
+    ps.stage = p;
+    ps.Yin = (p == 0) ? h.a.X : h.Y[p & 1];
+    ps.Yout = const_cast<double2*>(h.Y[(p + 1) & 1]);
+    ps.hg = c_G[11 - p];
+    ps.vscale = (p == 0) ? c_G[12] : 1.0;
+    ps.hlast = (p == 11) ? 1 : 0;
+    stage_tile<BN, NSTB, 2, 0>(h.a, ps, rtile * ncolt + ct, bsm);
+    __syncthreads();   // every thread's stores of the tile are issued
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(h.done + ((size_t)p * ncolt + ct) * g.nstate_blk + L, 1u);
+    }
+  }
+}
 
 // Stage-GEMM variants: pulse-column tile width (real columns), cp.async
 // pipeline depth, and whether the P and Q halves of a tile run in two CTAs
@@ -675,6 +796,37 @@ cudaError_t launch_variant(cudaStream_t st, int v, const StageArgs& a) {
   }
 }
 
+// The persistent Horner launch for tile variant v (its column width and ring
+// depth; a k-split variant runs unsplit): grid = min(work items, resident
+// CTAs), counters cleared on the stream first.
+template <int BN, int NST>
+cudaError_t launch_horner_tile(cudaStream_t st, const HornerArgs& h, int sms, int items) {
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_horner<BN, NST>,
+                                                                BTHREADS, batch_smem<BN, NST>());
+  if (e != cudaSuccess) return e;
+  const int grid = std::max(1, std::min(items, std::max(per_sm, 1) * sms));
+  // plain stream order: the counters' clear right before must be complete
+  k_batch_horner<BN, NST><<<grid, BTHREADS, batch_smem<BN, NST>(), st>>>(h);
+  return cudaGetLastError();
+}
+
+inline int horner_tile_bn(int v) { return kVariants[v].bn; }
+
+inline cudaError_t launch_horner_variant(cudaStream_t st, int v, const HornerArgs& h, int sms,
+                                         int items) {
+  switch (v) {
+    case 0: return launch_horner_tile<16, 3>(st, h, sms, items);
+    case 1:
+    case 5: return launch_horner_tile<16, 6>(st, h, sms, items);
+    case 2:
+    case 7: return launch_horner_tile<32, 3>(st, h, sms, items);
+    case 3:
+    case 6: return launch_horner_tile<32, 6>(st, h, sms, items);
+    default: return launch_horner_tile<64, 3>(st, h, sms, items);
+  }
+}
+
 // Workspace of the split variants for nrowtiles row tiles and ldc pulse
 // columns: two BM x BN partial tiles per tile pair, at most 2 ldc + 64 real
 // columns of tiles whatever BN is; the finest column tiling (16) sets the
@@ -704,6 +856,19 @@ cudaError_t set_stage_attrs() {
   MPC_STAGE_ATTR(32, 3, 1)
   MPC_STAGE_ATTR(64, 3, 1)
 #undef MPC_STAGE_ATTR
+  if (MODE == 2) {
+#define MPC_HORNER_ATTR(BN, NST)                                                          \
+  if ((e = cudaFuncSetAttribute(k_batch_horner<BN, NST>,                                  \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,             \
+                                batch_smem<BN, NST>())) != cudaSuccess)                  \
+    return e;
+    MPC_HORNER_ATTR(16, 3)
+    MPC_HORNER_ATTR(16, 6)
+    MPC_HORNER_ATTR(32, 3)
+    MPC_HORNER_ATTR(32, 6)
+    MPC_HORNER_ATTR(64, 3)
+#undef MPC_HORNER_ATTR
+  }
   return cudaSuccess;
 }
 
@@ -724,6 +889,7 @@ inline int stage_setup(int device) {
   CK(cudaMemcpyToSymbol(c_B8, B8, sizeof B8));
   CK(cudaMemcpyToSymbol(c_E, E, sizeof E));
   CK(cudaMemcpyToSymbol(c_C, Cn, sizeof Cn));
+  CK(cudaMemcpyToSymbol(c_G, rkf78::G, sizeof rkf78::G));
   CK(set_stage_attrs<0>());
   CK(set_stage_attrs<1>());
   CK(set_stage_attrs<2>());

@@ -100,6 +100,36 @@ def test_batched_resident_tail_barrier_timeout_is_reported():
     assert np.array_equal(X0, X1)
 
 
+def test_persistent_batched_step_dependency_timeout_is_reported():
+    """The batched fixed step's persistent launch (Horner products flowing
+    from one to the next on per-column progress counters): an injected
+    dependency that cannot complete runs out after the limit, the other CTAs
+    stop on the raised status, the call reports it, and the context recovers."""
+    from mpc_tdse.structure1e import hydrogen
+
+    # 1752 states (30 row tiles): 96 pulses give enough tiles per product for
+    # the persistent launch
+    s = hydrogen(n=300, k=9, R=200.0, l_max=5, gauge="l", states=[292] * 6)
+    Io, w = mpc_tdse.to_au(1e14, 1.5498)
+    tau = mpc_tdse.period(w, 1)
+    ps = [mpc_tdse.pulse_setup("sine", "l", Io * (1 + 0.01 * b), w, 0.0, 1, tau)
+          for b in range(96)]
+    X0 = np.zeros((96, s.ntot), complex)
+    X0[:, 0] = 1.0
+    steps = [30 + (b % 7) for b in range(96)]
+    with mpc_tdse.Context.from_system(s) as ctx:
+        ctx.set_path("streaming")   # every step on the GEMM path
+        Xa = ctx.batch_advance(ps, 0.0, 0.05, steps, X0)
+        ctx.set_wait_limit(1e-3)
+        ctx.inject_barrier_timeout()
+        with pytest.raises(mpc_tdse.MpcError) as ei:
+            ctx.batch_advance(ps, 0.0, 0.05, steps, X0)
+        assert ei.value.code == -3
+        ctx.set_wait_limit(2.0)
+        Xb = ctx.batch_advance(ps, 0.0, 0.05, steps, X0)
+    assert np.array_equal(Xa, Xb)
+
+
 @pytest.mark.parametrize("path", ["streaming", "resident"])
 def test_nan_in_host_state_raises_nonfinite_status(path):
     s = random_system([40, 57, 33], gauge="v", seed=11, e_max=4.0)
