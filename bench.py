@@ -460,6 +460,29 @@ def batched_kernel_case(local):
           f"resident 4 pulses: {int(acc4.sum() + rej4.sum())} pulse-attempts")
 
 
+def batched_ref_kernel_case(local):
+    """A short fixed-step batched run for profilers: the 256 pulses of the
+    batched workload, 6 steps each at dt 0.05 (one persistent Horner launch
+    per step), tile variant pinned to the one the tuner picks at 256 pulses on
+    a B200 (32-column tiles, 3-deep ring) and no tuning pass."""
+    import numpy as np
+
+    os.environ["MPC_NO_AUTOTUNE"] = "1"
+    os.environ["MPC_BATCH_VARIANT"] = "2"
+    import mpc_tdse
+    from mpc_tdse.structure1e import hydrogen
+
+    s = hydrogen(n=300, k=9, R=200.0, l_max=5, gauge="l", states=[292] * 6)
+    ctx = mpc_tdse.Context.from_system(s, device=local)
+    pulses, _ = batched_pulses(mpc_tdse)
+    X0 = np.zeros((len(pulses), s.ntot), complex)
+    X0[:, 0] = 1.0
+    X = ctx.batch_advance(pulses, 0.0, 0.05, [6] * len(pulses), X0)
+    ctx.close()
+    print(f"fixed-step batched: {len(pulses)} pulses x 6 steps, final norm "
+          f"{float(np.linalg.norm(X[0])):.15f}")
+
+
 def adjoint_kernel_case(local):
     """A short gradient for profilers: the adjoint workload's system, pulse
     and 4096 controls over the first 256 steps, checkpoint every 64 (one
@@ -795,7 +818,8 @@ def main():
     ap.add_argument("--no-he2e-batched", action="store_true",
                     help="skip the batched + adjoint 2e measurement (30k states, 64 pulses)")
     ap.add_argument("--mode", default="full",
-                    choices=["full", "kernel", "batched-kernel", "adjoint-kernel"],
+                    choices=["full", "kernel", "batched-kernel", "batched-ref-kernel",
+                             "adjoint-kernel"],
                     help="kernel: only warm-up + timed steps of the workload (a small case for "
                          "profilers); batched-kernel: a short batched run (256 pulses at full "
                          "width, then 4 pulses in the resident kernel) for profilers; "
@@ -812,6 +836,9 @@ def main():
         return
     if args.mode == "batched-kernel":
         batched_kernel_case(local)
+        return
+    if args.mode == "batched-ref-kernel":
+        batched_ref_kernel_case(local)
         return
     if args.mode == "adjoint-kernel":
         adjoint_kernel_case(local)
