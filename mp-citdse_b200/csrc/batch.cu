@@ -388,8 +388,7 @@ int launch_stage(mpc_ctx* c, const StageArgs& a) {
 // (k_batch_horner), when a product has enough tiles to fill the GPU; the
 // tile shape is the tuned variant's for this width.
 bool horner_persistent(mpc_ctx* c, int ncol) {
-  static const bool off = std::getenv("MPC_NO_PERSIST") != nullptr;
-  if (off) return false;
+  if (c->no_persist) return false;
   const int bn = horner_tile_bn(mpc_batch_variant(c, ncol));
   const int ncolt = (2 * ncol + bn - 1) / bn;
   return (long long)ncolt * c->batch->nrowtiles >= c->num_sms;

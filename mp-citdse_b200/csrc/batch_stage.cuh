@@ -801,10 +801,15 @@ cudaError_t launch_variant(cudaStream_t st, int v, const StageArgs& a) {
 // CTAs), counters cleared on the stream first.
 template <int BN, int NST>
 cudaError_t launch_horner_tile(cudaStream_t st, const HornerArgs& h, int sms, int items) {
-  int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_horner<BN, NST>,
-                                                                BTHREADS, batch_smem<BN, NST>());
-  if (e != cudaSuccess) return e;
+  static int per_sm = 0;   // resident CTAs per SM (the same on every B200)
+  if (per_sm == 0) {
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, k_batch_horner<BN, NST>, BTHREADS, batch_smem<BN, NST>());
+    if (e != cudaSuccess) {
+      per_sm = 0;
+      return e;
+    }
+  }
   const int grid = std::max(1, std::min(items, std::max(per_sm, 1) * sms));
   // plain stream order: the counters' clear right before must be complete
   k_batch_horner<BN, NST><<<grid, BTHREADS, batch_smem<BN, NST>(), st>>>(h);

@@ -77,6 +77,9 @@ struct mpc_ctx {
   // MPC_BATCH_VARIANT=v at context creation pins the stage-GEMM tile variant
   // (tests check that every variant gives the same bits); -1: tuned/default
   int forced_variant = -1;
+  // MPC_NO_PERSIST=1 at context creation: the batched fixed step as one launch
+  // per Horner product instead of the persistent launch
+  bool no_persist = false;
   // grid-barrier wait limit of the persistent kernels (mpc_ctx_set_wait_limit)
   unsigned long long wait_limit_ns = 2000000000ull;
   // the next persistent launch gets an unreachable barrier target

@@ -174,3 +174,32 @@ def test_batched_workload_pulses_match_reference():
     # the pre-renormalisation drift is RKF78's truncation at dt * rho <= 1.6
     # for the strongest pulses (2e-8 measured); it is stated, not pinned
     assert drift < 1e-6
+
+
+def test_persistent_step_equals_one_launch_per_product(monkeypatch):
+    """The persistent fixed-step launch (Horner products released tile by tile
+    on per-column progress counters) against one launch per product: the same
+    tiles with the same arithmetic, so the same bits; 96 pulses on the
+    benchmark system give enough tiles per product for the persistent launch,
+    uneven lengths exercise retirement and compaction in between."""
+    from mpc_tdse.structure1e import hydrogen
+
+    s = hydrogen(n=300, k=9, R=200.0, l_max=5, gauge="l", states=[292] * 6)
+    Io, w = mpc_tdse.to_au(2e14, 1.5498)
+    tau = mpc_tdse.period(w, 1)
+    ps = [mpc_tdse.pulse_setup("sine", "l", Io * (0.5 + 0.01 * b), w, 0.0, 1, tau)
+          for b in range(96)]
+    X0 = np.zeros((96, s.ntot), complex)
+    X0[:, 0] = 1.0
+    steps = [60 + 7 * (b % 13) for b in range(96)]
+    out = []
+    for persist in (True, False):
+        if not persist:
+            monkeypatch.setenv("MPC_NO_PERSIST", "1")
+        with mpc_tdse.Context.from_system(s) as ctx:
+            ctx.set_path("streaming")
+            out.append(ctx.batch_advance(ps, 0.0, 0.05, steps, X0, history=True))
+    (X1, p1, n1), (X2, p2, n2) = out
+    assert np.array_equal(X1, X2)
+    assert np.array_equal(p1, p2)
+    assert np.array_equal(n1, n2)
