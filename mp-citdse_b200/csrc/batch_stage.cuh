@@ -49,6 +49,15 @@ template <int BN_> constexpr int b_stage() { return BK * (BN_ + 4); }
 template <int BN_, int NST_> constexpr int batch_smem() {
   return NST_ * (A_STAGE + b_stage<BN_>()) * 8;
 }
+// Unsplit variants with narrow tiles pair each P chunk with the Q chunk of
+// the same index in one ring slot (see stage_tile): NST_ chunk slots become
+// 2 (NST_ = 3) or 3 (NST_ = 6) slots of two chunks.
+template <int BN_, int SPLIT_> constexpr bool paired() { return SPLIT_ == 0 && BN_ <= 32; }
+template <int NST_> constexpr int pair_slots() { return NST_ >= 6 ? 3 : 2; }
+template <int BN_, int NST_, int SPLIT_> constexpr int stage_smem() {
+  return paired<BN_, SPLIT_>() ? pair_slots<NST_>() * 2 * (A_STAGE + b_stage<BN_>()) * 8
+                               : batch_smem<BN_, NST_>();
+}
 
 __constant__ double c_A[13][13];
 __constant__ double c_B8[13];
@@ -183,6 +192,72 @@ __device__ __forceinline__ ProdSel prod_sel(const StageArgs& a) {
   return ProdSel{a.Yin, a.Yout, a.stage, a.hg, a.vscale, a.hlast};
 }
 
+// A P chunk and a Q chunk of the same index together: per 8-deep k-step the
+// P product goes into accP and the Q product into accQ, so each warp keeps
+// twice as many independent DMMA accumulations in flight as with one chunk
+// at a time, with each accumulator's terms in the same order as before.
+template <int BN>
+__device__ __forceinline__ void pair_mma(const double* AsP, const double* BsP, const double* AsQ,
+                                         const double* BsQ, int wm, int wn, int gq, int tq,
+                                         double sign, int nksP, int nksQ, int mt_lim,
+                                         double (&accP)[Tile<BN>::WMT][Tile<BN>::WNT][4],
+                                         double (&accQ)[Tile<BN>::WMT][Tile<BN>::WNT][4]) {
+  constexpr int WMT = Tile<BN>::WMT, WNT = Tile<BN>::WNT;
+  constexpr int LDB = BN + 4;
+#pragma unroll
+  for (int ks = 0; ks < BK / 8; ++ks) {
+    const int k = ks * 8 + tq;
+    if (ks < nksP) {
+      double af[WMT][4], bf[WNT][2];
+#pragma unroll
+      for (int mt = 0; mt < WMT; ++mt) {
+        if (mt >= mt_lim) break;
+        const int m = wm * (WMT * 16) + mt * 16 + gq;
+        af[mt][0] = AsP[k * LDA_P + m];
+        af[mt][1] = AsP[k * LDA_P + m + 8];
+        af[mt][2] = AsP[(k + 4) * LDA_P + m];
+        af[mt][3] = AsP[(k + 4) * LDA_P + m + 8];
+      }
+#pragma unroll
+      for (int nt = 0; nt < WNT; ++nt) {
+        const int n = wn * (WNT * 8) + nt * 8 + gq;
+        bf[nt][0] = BsP[k * LDB + n];
+        bf[nt][1] = BsP[(k + 4) * LDB + n];
+      }
+#pragma unroll
+      for (int mt = 0; mt < WMT; ++mt) {
+        if (mt >= mt_lim) break;
+#pragma unroll
+        for (int nt = 0; nt < WNT; ++nt) dmma16x8x8(accP[mt][nt], af[mt], bf[nt]);
+      }
+    }
+    if (ks < nksQ) {
+      double af[WMT][4], bf[WNT][2];
+#pragma unroll
+      for (int mt = 0; mt < WMT; ++mt) {
+        if (mt >= mt_lim) break;
+        const int m = wm * (WMT * 16) + mt * 16 + gq;
+        af[mt][0] = sign * AsQ[m * LDA_Q + k];
+        af[mt][1] = sign * AsQ[(m + 8) * LDA_Q + k];
+        af[mt][2] = sign * AsQ[m * LDA_Q + k + 4];
+        af[mt][3] = sign * AsQ[(m + 8) * LDA_Q + k + 4];
+      }
+#pragma unroll
+      for (int nt = 0; nt < WNT; ++nt) {
+        const int n = wn * (WNT * 8) + nt * 8 + gq;
+        bf[nt][0] = BsQ[k * LDB + n];
+        bf[nt][1] = BsQ[(k + 4) * LDB + n];
+      }
+#pragma unroll
+      for (int mt = 0; mt < WMT; ++mt) {
+        if (mt >= mt_lim) break;
+#pragma unroll
+        for (int nt = 0; nt < WNT; ++nt) dmma16x8x8(accQ[mt][nt], af[mt], bf[nt]);
+      }
+    }
+  }
+}
+
 template <int BN, int NSTB, int MODE, int SPLIT>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, const ProdSel& ps, const int bid,
                                            double* bsm) {
@@ -249,8 +324,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const ProdSel& ps
   const double* q_base = hasQ ? a.D + g.blk[L].d_off + (long long)(r0 + q_mm0) * pitchQ + q_kk : a.D;
   const int yrowP = hasP ? g.state_off[L - 1] : 0, yrowQ = hasQ ? g.state_off[L + 1] : 0;
 
-  auto load_chunk = [&](int ch, int st) {
-    double* As = bsm + st * (A_STAGE + B_STAGE);
+  auto load_chunk = [&](int ch, double* As) {
     double* Bs = As + A_STAGE;
     const bool isP = ch < nchP;
     const int k0 = (isP ? ch : ch - nchP) * BK;
@@ -297,35 +371,67 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const ProdSel& ps
 #pragma unroll
       for (int v = 0; v < 4; ++v) accP[i][j][v] = accQ[i][j][v] = 0.0;
 
-  const int ch0 = (SPLIT && zk == 1) ? nchP : 0;
-  const int ch1 = (SPLIT && zk == 0) ? nchP : nch;
-  const int nmine = ch1 - ch0;
-  for (int p = 0; p < NSTB - 1; ++p) {
-    if (p < nmine) load_chunk(ch0 + p, p);
-    cp_commit();
-  }
-  // this CTA's P chunks come first (local indices [0, nPm)), then its Q chunks
-  const int nPm = (SPLIT && zk == 1) ? 0 : nchP;
-  for (int ci = 0; ci < nmine; ++ci) {
-    cp_wait<NSTB - 2>();
-    __syncthreads();
-    {
-      const int nx = ci + NSTB - 1;
-      if (nx < nmine) load_chunk(ch0 + nx, nx % NSTB);
+  if constexpr (paired<BN, SPLIT>()) {
+    // slot i holds P chunk i (first half) and Q chunk i (second half)
+    constexpr int NSP = pair_slots<NSTB>();
+    constexpr int CH = A_STAGE + B_STAGE;
+    const int nsup = max(nchP, nchQ);
+    auto load_pair = [&](int i, int slot) {
+      double* base = bsm + slot * 2 * CH;
+      if (i < nchP) load_chunk(i, base);
+      if (i < nchQ) load_chunk(nchP + i, base + CH);
+    };
+    for (int p = 0; p < NSP - 1; ++p) {
+      if (p < nsup) load_pair(p, p);
       cp_commit();
     }
-    const double* As = bsm + (ci % NSTB) * (A_STAGE + B_STAGE);
-    const double* Bs = As + A_STAGE;
-    // valid k-steps of this chunk: the coupled block's columns left from k0
-    const int chg = ch0 + ci;
-    const int krem = (chg < nchP) ? KP - chg * BK : KQ - (chg - nchP) * BK;
-    const int nks = min(BK / 8, (krem + 7) / 8);
-    if (ci < nPm)
-      chunk_mma<BN, true>(As, Bs, wm, wn, gq, tq, 1.0, nks, mt_lim, accP);
-    else
-      chunk_mma<BN, false>(As, Bs, wm, wn, gq, tq, qsign, nks, mt_lim, accQ);
+    for (int i = 0; i < nsup; ++i) {
+      cp_wait<NSP - 2>();
+      __syncthreads();
+      {
+        const int nx = i + NSP - 1;
+        if (nx < nsup) load_pair(nx, nx % NSP);
+        cp_commit();
+      }
+      const double* base = bsm + (i % NSP) * 2 * CH;
+      // valid k-steps: the coupled blocks' columns left from k0 = i * BK
+      const int nksP = i < nchP ? min(BK / 8, (KP - i * BK + 7) / 8) : 0;
+      const int nksQ = i < nchQ ? min(BK / 8, (KQ - i * BK + 7) / 8) : 0;
+      pair_mma<BN>(base, base + A_STAGE, base + CH, base + CH + A_STAGE, wm, wn, gq, tq, qsign,
+                   nksP, nksQ, mt_lim, accP, accQ);
+    }
+    cp_wait<0>();
+  } else {
+    const int ch0 = (SPLIT && zk == 1) ? nchP : 0;
+    const int ch1 = (SPLIT && zk == 0) ? nchP : nch;
+    const int nmine = ch1 - ch0;
+    for (int p = 0; p < NSTB - 1; ++p) {
+      if (p < nmine) load_chunk(ch0 + p, bsm + p * (A_STAGE + B_STAGE));
+      cp_commit();
+    }
+    // this CTA's P chunks come first (local indices [0, nPm)), then its Q chunks
+    const int nPm = (SPLIT && zk == 1) ? 0 : nchP;
+    for (int ci = 0; ci < nmine; ++ci) {
+      cp_wait<NSTB - 2>();
+      __syncthreads();
+      {
+        const int nx = ci + NSTB - 1;
+        if (nx < nmine) load_chunk(ch0 + nx, bsm + (nx % NSTB) * (A_STAGE + B_STAGE));
+        cp_commit();
+      }
+      const double* As = bsm + (ci % NSTB) * (A_STAGE + B_STAGE);
+      const double* Bs = As + A_STAGE;
+      // valid k-steps of this chunk: the coupled block's columns left from k0
+      const int chg = ch0 + ci;
+      const int krem = (chg < nchP) ? KP - chg * BK : KQ - (chg - nchP) * BK;
+      const int nks = min(BK / 8, (krem + 7) / 8);
+      if (ci < nPm)
+        chunk_mma<BN, true>(As, Bs, wm, wn, gq, tq, 1.0, nks, mt_lim, accP);
+      else
+        chunk_mma<BN, false>(As, Bs, wm, wn, gq, tq, qsign, nks, mt_lim, accQ);
+    }
+    cp_wait<0>();
   }
-  cp_wait<0>();
   if constexpr (SPLIT) {
     // publish this half, then the tile's second arrival takes over
     constexpr int NACC = WM_TILES * WN_TILES * 4;
@@ -778,7 +884,7 @@ cudaError_t launch_tile(cudaStream_t st, const StageArgs& a) {
   const int ncolt = (2 * a.ncol + BN - 1) / BN;
   return mpc_launch_pdl(k_batch_stage<BN, NST, MODE, SPLIT>,
                         dim3(a.nrowtiles * ncolt * (SPLIT ? 2 : 1)), dim3(BTHREADS),
-                        batch_smem<BN, NST>(), st, a);
+                        stage_smem<BN, NST, SPLIT>(), st, a);
 }
 
 template <int MODE>
@@ -804,7 +910,7 @@ cudaError_t launch_horner_tile(cudaStream_t st, const HornerArgs& h, int sms, in
   static int per_sm = 0;   // resident CTAs per SM (the same on every B200)
   if (per_sm == 0) {
     const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, k_batch_horner<BN, NST>, BTHREADS, batch_smem<BN, NST>());
+        &per_sm, k_batch_horner<BN, NST>, BTHREADS, stage_smem<BN, NST, 0>());
     if (e != cudaSuccess) {
       per_sm = 0;
       return e;
@@ -812,7 +918,7 @@ cudaError_t launch_horner_tile(cudaStream_t st, const HornerArgs& h, int sms, in
   }
   const int grid = std::max(1, std::min(items, std::max(per_sm, 1) * sms));
   // plain stream order: the counters' clear right before must be complete
-  k_batch_horner<BN, NST><<<grid, BTHREADS, batch_smem<BN, NST>(), st>>>(h);
+  k_batch_horner<BN, NST><<<grid, BTHREADS, stage_smem<BN, NST, 0>(), st>>>(h);
   return cudaGetLastError();
 }
 
@@ -849,7 +955,7 @@ cudaError_t set_stage_attrs() {
 #define MPC_STAGE_ATTR(BN, NST, SPLIT)                                                   \
   if ((e = cudaFuncSetAttribute(k_batch_stage<BN, NST, MODE, SPLIT>,                     \
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,             \
-                                batch_smem<BN, NST>())) != cudaSuccess)                  \
+                                stage_smem<BN, NST, SPLIT>())) != cudaSuccess)           \
     return e;
   MPC_STAGE_ATTR(16, 3, 0)
   MPC_STAGE_ATTR(16, 6, 0)
@@ -865,7 +971,7 @@ cudaError_t set_stage_attrs() {
 #define MPC_HORNER_ATTR(BN, NST)                                                          \
   if ((e = cudaFuncSetAttribute(k_batch_horner<BN, NST>,                                  \
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,             \
-                                batch_smem<BN, NST>())) != cudaSuccess)                  \
+                                stage_smem<BN, NST, 0>())) != cudaSuccess)               \
     return e;
     MPC_HORNER_ATTR(16, 3)
     MPC_HORNER_ATTR(16, 6)
