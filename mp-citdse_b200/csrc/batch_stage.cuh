@@ -127,14 +127,18 @@ struct StageArgs {
 
 
 // One BK-deep chunk of the tile product from shared memory into acc: the A
-// operand is D_{L-1}^T (IS_P, stored k-major) or sign * D_L (stored m-major).
+// operand is D_{L-1}^T (IS_P, stored k-major) or D_L (stored m-major).  The
+// velocity gauge's minus sign on the D_L term is applied once to its
+// accumulated sum: negation commutes exactly with every rounding, so
+// sign * sum(D y) has the bits of sum((sign D) y), without a multiply between
+// each fragment load and its DMMA.
 // Only the chunk's first nks 8-deep k-steps hold coupling (the rest of the
 // last chunk of a block is zero fill) and only this warp's first mt_lim
 // 16-row m-tiles hold rows of the block: the rest would add exact zeros or
 // rows that are never stored, so they are skipped (warp-uniform branches).
 template <int BN, bool IS_P>
 __device__ __forceinline__ void chunk_mma(const double* As, const double* Bs, int wm, int wn,
-                                          int gq, int tq, double sign, int nks, int mt_lim,
+                                          int gq, int tq, int nks, int mt_lim,
                                           double (&acc)[Tile<BN>::WMT][Tile<BN>::WNT][4]) {
   constexpr int WMT = Tile<BN>::WMT, WNT = Tile<BN>::WNT;
   constexpr int LDB = BN + 4;
@@ -153,10 +157,10 @@ __device__ __forceinline__ void chunk_mma(const double* As, const double* Bs, in
         af[mt][2] = As[(k + 4) * LDA_P + m];
         af[mt][3] = As[(k + 4) * LDA_P + m + 8];
       } else {
-        af[mt][0] = sign * As[m * LDA_Q + k];
-        af[mt][1] = sign * As[(m + 8) * LDA_Q + k];
-        af[mt][2] = sign * As[m * LDA_Q + k + 4];
-        af[mt][3] = sign * As[(m + 8) * LDA_Q + k + 4];
+        af[mt][0] = As[m * LDA_Q + k];
+        af[mt][1] = As[(m + 8) * LDA_Q + k];
+        af[mt][2] = As[m * LDA_Q + k + 4];
+        af[mt][3] = As[(m + 8) * LDA_Q + k + 4];
       }
     }
 #pragma unroll
@@ -199,7 +203,7 @@ __device__ __forceinline__ ProdSel prod_sel(const StageArgs& a) {
 template <int BN>
 __device__ __forceinline__ void pair_mma(const double* AsP, const double* BsP, const double* AsQ,
                                          const double* BsQ, int wm, int wn, int gq, int tq,
-                                         double sign, int nksP, int nksQ, int mt_lim,
+                                         int nksP, int nksQ, int mt_lim,
                                          double (&accP)[Tile<BN>::WMT][Tile<BN>::WNT][4],
                                          double (&accQ)[Tile<BN>::WMT][Tile<BN>::WNT][4]) {
   constexpr int WMT = Tile<BN>::WMT, WNT = Tile<BN>::WNT;
@@ -237,10 +241,10 @@ __device__ __forceinline__ void pair_mma(const double* AsP, const double* BsP, c
       for (int mt = 0; mt < WMT; ++mt) {
         if (mt >= mt_lim) break;
         const int m = wm * (WMT * 16) + mt * 16 + gq;
-        af[mt][0] = sign * AsQ[m * LDA_Q + k];
-        af[mt][1] = sign * AsQ[(m + 8) * LDA_Q + k];
-        af[mt][2] = sign * AsQ[m * LDA_Q + k + 4];
-        af[mt][3] = sign * AsQ[(m + 8) * LDA_Q + k + 4];
+        af[mt][0] = AsQ[m * LDA_Q + k];
+        af[mt][1] = AsQ[(m + 8) * LDA_Q + k];
+        af[mt][2] = AsQ[m * LDA_Q + k + 4];
+        af[mt][3] = AsQ[(m + 8) * LDA_Q + k + 4];
       }
 #pragma unroll
       for (int nt = 0; nt < WNT; ++nt) {
@@ -397,8 +401,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const ProdSel& ps
       // valid k-steps: the coupled blocks' columns left from k0 = i * BK
       const int nksP = i < nchP ? min(BK / 8, (KP - i * BK + 7) / 8) : 0;
       const int nksQ = i < nchQ ? min(BK / 8, (KQ - i * BK + 7) / 8) : 0;
-      pair_mma<BN>(base, base + A_STAGE, base + CH, base + CH + A_STAGE, wm, wn, gq, tq, qsign,
-                   nksP, nksQ, mt_lim, accP, accQ);
+      pair_mma<BN>(base, base + A_STAGE, base + CH, base + CH + A_STAGE, wm, wn, gq, tq, nksP,
+                   nksQ, mt_lim, accP, accQ);
     }
     cp_wait<0>();
   } else {
@@ -426,9 +430,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const ProdSel& ps
       const int krem = (chg < nchP) ? KP - chg * BK : KQ - (chg - nchP) * BK;
       const int nks = min(BK / 8, (krem + 7) / 8);
       if (ci < nPm)
-        chunk_mma<BN, true>(As, Bs, wm, wn, gq, tq, 1.0, nks, mt_lim, accP);
+        chunk_mma<BN, true>(As, Bs, wm, wn, gq, tq, nks, mt_lim, accP);
       else
-        chunk_mma<BN, false>(As, Bs, wm, wn, gq, tq, qsign, nks, mt_lim, accQ);
+        chunk_mma<BN, false>(As, Bs, wm, wn, gq, tq, nks, mt_lim, accQ);
     }
     cp_wait<0>();
   }
@@ -475,7 +479,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const ProdSel& ps
 #pragma unroll
     for (int j = 0; j < WN_TILES; ++j)
 #pragma unroll
-      for (int v = 0; v < 4; ++v) acc[i][j][v] = accP[i][j][v] + accQ[i][j][v];
+      for (int v = 0; v < 4; ++v) acc[i][j][v] = accP[i][j][v] + qsign * accQ[i][j][v];
 
   if constexpr (MODE == 2) {
     // ---------------- Horner epilogue (fixed step, frozen field) ----------------
