@@ -323,6 +323,7 @@ def measure_batched_ref(local, stream_cls, rank=0, world=1, dist=None, dt=0.05):
     # warm-up at full width (graph capture per width, module loads)
     ctx.batch_advance(pulses, 0.0, dt, [40] * B, X0)
     ctx.sync()
+    plan = ctx.batch_fixed_plan()
     e0.record(st)
     X = ctx.batch_advance(pulses, 0.0, dt, steps, X0)
     e1.record(st)
@@ -382,6 +383,8 @@ def measure_batched_ref(local, stream_cls, rank=0, world=1, dist=None, dt=0.05):
                                       "graphs on)" % (B, fw_steps)},
         "tiles": [{"pulses": a, "tile_cols": b, "stages": c, "k_split": d, "us_per_rhs": e}
                   for a, b, c, d, e in tiles],
+        "step_plan": [{"pulses": a, "persistent": bool(b), "tile_cols": c, "ring": d,
+                       "us_per_step": e} for a, b, c, d, e in plan],
         "roofline": {"bound": "tensor", "achieved": live_tflops, "peak": dmma, "unit": "TFLOP/s",
                      "frac": live_tflops / dmma, "kernel": "k_batch_stage",
                      "measured_on": "whole steps at full width (%d pulses x %d steps, graph "

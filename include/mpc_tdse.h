@@ -227,6 +227,15 @@ int mpc_propagate_batch(mpc_ctx *ctx, int B, const mpc_pulse *pulses, const doub
  * Returns the number of rows (>= 0) or an error code. */
 int mpc_batch_autotune(mpc_ctx *ctx, int B, double *table, int cap);
 
+/* How the batched fixed step (mpc_batch_advance) ran at each width: on its
+ * first use the library times, at widths 1, 2, 4, ... pulses, a whole step
+ * as one launch per Horner product and as one persistent launch on each
+ * unsplit tile shape, and keeps the fastest (every choice gives the same
+ * bits).  Rows of 5 doubles, up to cap: pulses, persistent (1) or one launch
+ * per product (0), tile width (real columns), ring depth, microseconds per
+ * step.  Returns the number of rows (0 before any fixed-step call). */
+int mpc_batch_fixed_plan(mpc_ctx *ctx, double *table, int cap);
+
 /* Objective and gradient (new: the reference has no gradients).
  *
  * The field of the fixed-step propagation (mpc_propagate semantics: F frozen

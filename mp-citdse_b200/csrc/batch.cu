@@ -290,6 +290,11 @@ struct mpc_batch_state {
   // autotuned stage-GEMM variant per width bucket (bucket j: up to 2^j pulses)
   std::vector<int> tile;
   std::vector<double> tile_us;
+  // fixed-step steps, per width bucket: -1 one launch per Horner product
+  // (with the tuned variant), v >= 0 the persistent launch on variant v;
+  // microseconds per step of the choice
+  std::vector<int> hplan;
+  std::vector<double> hplan_us;
 };
 
 namespace {
@@ -384,19 +389,25 @@ int launch_stage(mpc_ctx* c, const StageArgs& a) {
   return MPC_OK;
 }
 
-// The 12 Horner products of a fixed step in one persistent launch
-// (k_batch_horner), when a product has enough tiles to fill the GPU; the
-// tile shape is the tuned variant's for this width.
-bool horner_persistent(mpc_ctx* c, int ncol) {
-  if (c->no_persist) return false;
-  const int bn = horner_tile_bn(mpc_batch_variant(c, ncol));
+// How a fixed step of ncol pulses runs: -1 one launch per Horner product,
+// else the persistent launch (k_batch_horner) on tile variant v.  The
+// fixed-step tuner's choice when it ran; otherwise persistent on the tuned
+// variant when a product has enough tiles to fill the GPU.
+int horner_plan(mpc_ctx* c, int ncol) {
+  if (c->no_persist) return -1;
+  const mpc_batch_state* b = c->batch;
+  const int j = width_bucket(ncol);
+  if (j < (int)b->hplan.size()) return b->hplan[j];
+  const int v = mpc_batch_variant(c, ncol);
+  const int bn = horner_tile_bn(v);
   const int ncolt = (2 * ncol + bn - 1) / bn;
-  return (long long)ncolt * c->batch->nrowtiles >= c->num_sms;
+  return (long long)ncolt * b->nrowtiles >= c->num_sms ? v : -1;
 }
 
-int launch_horner_persistent(mpc_ctx* c, int ncol) {
+bool horner_persistent(mpc_ctx* c, int ncol) { return horner_plan(c, ncol) >= 0; }
+
+int launch_horner_persistent_v(mpc_ctx* c, int ncol, int v) {
   mpc_batch_state* b = c->batch;
-  const int v = mpc_batch_variant(c, ncol);
   const int bn = horner_tile_bn(v);
   HornerArgs h{};
   h.a = stage_args(c, 0, ncol, 1.0, 1.0, false);
@@ -416,6 +427,10 @@ int launch_horner_persistent(mpc_ctx* c, int ncol) {
   ++c->launches;
   CK(launch_horner_variant(c->stream, v, h, c->num_sms, items));
   return MPC_OK;
+}
+
+int launch_horner_persistent(mpc_ctx* c, int ncol) {
+  return launch_horner_persistent_v(c, ncol, horner_plan(c, ncol));
 }
 
 // Product p = 0 .. 11 of a fixed-step (frozen-field) step evaluated as the
@@ -481,6 +496,64 @@ int autotune(mpc_ctx* c, int max_cols) {
   return MPC_OK;
 }
 
+// The fixed-step tuner: at widths 1, 2, 4, ... up to max_cols pulses, times
+// one whole step's 12 Horner products as one launch per product (on the
+// tuned variant) and as the persistent launch on each unsplit tile shape,
+// and keeps the fastest.  Every candidate computes the same tiles in the same
+// order, so the choice changes speed only.  Runs on the batch's work
+// buffers before the propagation loads its states.
+int autotune_horner(mpc_ctx* c, int max_cols) {
+  mpc_batch_state* b = c->batch;
+  const int top = width_bucket(std::min(std::max(max_cols, 1), b->ldc));
+  std::vector<int> plan(top + 1, -1);
+  std::vector<double> plan_us(top + 1, 0.0);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int cands[] = {-1, 0, 1, 2, 3, 4};
+  int rc = MPC_OK;
+  const long long l0 = c->launches;
+  for (int j = 0; j <= top && rc == MPC_OK; ++j) {
+    const int w = std::min(1 << j, b->ldc);
+    double best = 1e300;
+    for (int v : cands) {
+      auto step = [&]() -> int {
+        if (v < 0) {
+          for (int p = 0; p < 12; ++p) {
+            int r = launch_horner(c, p, w);
+            if (r) return r;
+          }
+          return MPC_OK;
+        }
+        return launch_horner_persistent_v(c, w, v);
+      };
+      for (int r = 0; r < 2 && rc == MPC_OK; ++r) rc = step();
+      if (rc) break;
+      CK(cudaEventRecord(e0, c->stream));
+      const int reps = 3;
+      for (int r = 0; r < reps && rc == MPC_OK; ++r) rc = step();
+      if (rc) break;
+      CK(cudaEventRecord(e1, c->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      const double t = 1000.0 * ms / reps;
+      if (t < best) {
+        best = t;
+        plan[j] = v;
+        plan_us[j] = t;
+      }
+    }
+  }
+  c->launches = l0;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  b->hplan = plan;
+  b->hplan_us = plan_us;
+  return MPC_OK;
+}
+
 }  // namespace
 
 int mpc_batch_variant(mpc_ctx* c, int ncol) {
@@ -538,6 +611,23 @@ int mpc_propagate_batch(mpc_ctx* c, int B, const mpc_pulse* pulses, const double
                         double* t_final) {
   return mpc_batch_propagate(c, B, pulses, t0, t_end, h0, dt_max, rtol, atol, max_attempts, ct,
                              accepted, rejected, t_final);
+}
+
+int mpc_batch_fixed_plan(mpc_ctx* c, double* table, int cap) {
+  if (!c || (table && cap < 0)) return mpc_fail(MPC_ERR_ARG, "bad argument");
+  if (!c->batch || c->batch->hplan.empty()) return 0;
+  const mpc_batch_state* b = c->batch;
+  const int rows = (int)b->hplan.size();
+  for (int j = 0; table && j < rows && j < cap; ++j) {
+    const int v = b->hplan[j];
+    const int vv = v >= 0 ? v : mpc_batch_variant(c, std::min(1 << j, b->ldc));
+    table[5 * j + 0] = std::min(1 << j, b->ldc);
+    table[5 * j + 1] = v >= 0 ? 1 : 0;
+    table[5 * j + 2] = kVariants[vv].bn;
+    table[5 * j + 3] = v >= 0 ? (kVariants[vv].nst >= 6 ? 3 : 2) : kVariants[vv].nst;
+    table[5 * j + 4] = b->hplan_us[j];
+  }
+  return rows;
 }
 
 int mpc_batch_autotune(mpc_ctx* c, int B, double* table, int cap) {
@@ -699,6 +789,9 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
   };
 
   if (b->tile.empty() && !std::getenv("MPC_NO_AUTOTUNE") && (rc = autotune(c, B))) return rc;
+  if (fx.on && b->hplan.empty() && !c->no_persist && !std::getenv("MPC_NO_AUTOTUNE") &&
+      (rc = autotune_horner(c, B)))
+    return rc;
 
   // One attempted step of every active pulse: 13 stage GEMMs, the step
   // controller, the accepted-state update and the retirement flags.

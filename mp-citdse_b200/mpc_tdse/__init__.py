@@ -100,6 +100,7 @@ def lib():
     L.mpc_batch_objective_backward.argtypes = [C.c_void_p, _dp, _dp]
     L.mpc_batch_objective_info.argtypes = [C.c_void_p, _ip, _ip, _dp]
     L.mpc_batch_autotune.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]
+    L.mpc_batch_fixed_plan.argtypes = [C.c_void_p, _dp, C.c_int]
     L.mpc_batch_propagate.argtypes = [C.c_void_p, C.c_int, C.POINTER(Pulse), _dp, _dp, C.c_double,
                                       C.c_double, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
                                       _dp]
@@ -293,6 +294,15 @@ class Context:
         cap = 32
         tab = np.zeros((cap, 5))
         r = lib().mpc_batch_autotune(self._h, int(B), _ptr(tab), cap)
+        _check(min(r, 0))
+        return [(int(a), int(b), int(c), int(d), float(e)) for a, b, c, d, e in tab[:r]]
+
+    def batch_fixed_plan(self):
+        """Rows of (pulses, persistent, tile width, ring depth, us per step)
+        chosen for the batched fixed step."""
+        cap = 32
+        tab = np.zeros((cap, 5))
+        r = lib().mpc_batch_fixed_plan(self._h, _ptr(tab), cap)
         _check(min(r, 0))
         return [(int(a), int(b), int(c), int(d), float(e)) for a, b, c, d, e in tab[:r]]
 
