@@ -192,6 +192,9 @@ def test_persistent_step_equals_one_launch_per_product(monkeypatch):
     X0 = np.zeros((96, s.ntot), complex)
     X0[:, 0] = 1.0
     steps = [60 + 7 * (b % 13) for b in range(96)]
+    # untuned: the persistent launch whenever a product fills the GPU (the
+    # tuner might otherwise pick one launch per product at every width)
+    monkeypatch.setenv("MPC_NO_AUTOTUNE", "1")
     out = []
     for persist in (True, False):
         if not persist:

@@ -100,7 +100,7 @@ def test_batched_resident_tail_barrier_timeout_is_reported():
     assert np.array_equal(X0, X1)
 
 
-def test_persistent_batched_step_dependency_timeout_is_reported():
+def test_persistent_batched_step_dependency_timeout_is_reported(monkeypatch):
     """The batched fixed step's persistent launch (Horner products flowing
     from one to the next on per-column progress counters): an injected
     dependency that cannot complete runs out after the limit, the other CTAs
@@ -117,6 +117,8 @@ def test_persistent_batched_step_dependency_timeout_is_reported():
     X0 = np.zeros((96, s.ntot), complex)
     X0[:, 0] = 1.0
     steps = [30 + (b % 7) for b in range(96)]
+    # untuned: the persistent launch whenever a product fills the GPU
+    monkeypatch.setenv("MPC_NO_AUTOTUNE", "1")
     with mpc_tdse.Context.from_system(s) as ctx:
         ctx.set_path("streaming")   # every step on the GEMM path
         Xa = ctx.batch_advance(ps, 0.0, 0.05, steps, X0)
