@@ -396,6 +396,7 @@ int launch_stage(mpc_ctx* c, const StageArgs& a) {
 int horner_plan(mpc_ctx* c, int ncol) {
   if (c->no_persist) return -1;
   const mpc_batch_state* b = c->batch;
+  if (c->force_persist) return mpc_batch_variant(c, ncol);
   const int j = width_bucket(ncol);
   if (j < (int)b->hplan.size()) return b->hplan[j];
   const int v = mpc_batch_variant(c, ncol);
@@ -789,7 +790,8 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
   };
 
   if (b->tile.empty() && !std::getenv("MPC_NO_AUTOTUNE") && (rc = autotune(c, B))) return rc;
-  if (fx.on && b->hplan.empty() && !c->no_persist && !std::getenv("MPC_NO_AUTOTUNE") &&
+  if (fx.on && b->hplan.empty() && !c->no_persist && !c->force_persist &&
+      !std::getenv("MPC_NO_AUTOTUNE") &&
       (rc = autotune_horner(c, B)))
     return rc;
 

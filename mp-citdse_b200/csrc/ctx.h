@@ -80,6 +80,9 @@ struct mpc_ctx {
   // MPC_NO_PERSIST=1 at context creation: the batched fixed step as one launch
   // per Horner product instead of the persistent launch
   bool no_persist = false;
+  // MPC_FORCE_PERSIST=1 at context creation: the persistent launch at every
+  // width (tests of that path; it is correct at any width, not always faster)
+  bool force_persist = false;
   // grid-barrier wait limit of the persistent kernels (mpc_ctx_set_wait_limit)
   unsigned long long wait_limit_ns = 2000000000ull;
   // the next persistent launch gets an unreachable barrier target

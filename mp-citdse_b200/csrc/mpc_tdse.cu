@@ -494,6 +494,7 @@ int mpc_ctx_create(int L_max, const int* state_sz, const double* eig, const doub
   c->device = device;
   if (const char* v = std::getenv("MPC_BATCH_VARIANT")) c->forced_variant = std::atoi(v);
   c->no_persist = std::getenv("MPC_NO_PERSIST") != nullptr;
+  c->force_persist = std::getenv("MPC_FORCE_PERSIST") != nullptr;
   c->gauge = gauge;
   c->n.assign(state_sz, state_sz + L_max + 1);
   CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));

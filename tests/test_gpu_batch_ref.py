@@ -192,13 +192,12 @@ def test_persistent_step_equals_one_launch_per_product(monkeypatch):
     X0 = np.zeros((96, s.ntot), complex)
     X0[:, 0] = 1.0
     steps = [60 + 7 * (b % 13) for b in range(96)]
-    # untuned: the persistent launch whenever a product fills the GPU (the
-    # tuner might otherwise pick one launch per product at every width)
-    monkeypatch.setenv("MPC_NO_AUTOTUNE", "1")
     out = []
     for persist in (True, False):
+        # the persistent launch at every width, then one launch per product
+        monkeypatch.setenv("MPC_FORCE_PERSIST" if persist else "MPC_NO_PERSIST", "1")
         if not persist:
-            monkeypatch.setenv("MPC_NO_PERSIST", "1")
+            monkeypatch.delenv("MPC_FORCE_PERSIST")
         with mpc_tdse.Context.from_system(s) as ctx:
             ctx.set_path("streaming")
             out.append(ctx.batch_advance(ps, 0.0, 0.05, steps, X0, history=True))

@@ -117,8 +117,8 @@ def test_persistent_batched_step_dependency_timeout_is_reported(monkeypatch):
     X0 = np.zeros((96, s.ntot), complex)
     X0[:, 0] = 1.0
     steps = [30 + (b % 7) for b in range(96)]
-    # untuned: the persistent launch whenever a product fills the GPU
-    monkeypatch.setenv("MPC_NO_AUTOTUNE", "1")
+    # the persistent launch at every width
+    monkeypatch.setenv("MPC_FORCE_PERSIST", "1")
     with mpc_tdse.Context.from_system(s) as ctx:
         ctx.set_path("streaming")   # every step on the GEMM path
         Xa = ctx.batch_advance(ps, 0.0, 0.05, steps, X0)
