@@ -52,6 +52,11 @@ struct ControlArgs {
   int max_attempts;
   FixedStep fx;               // fixed-step mode (the reference's semantics)
   unsigned* status;
+  // fixed-step mode: the step's unnormalised x_new [n][ldc] (the next step's
+  // first product normalises it); a pulse that finishes is written out here
+  const double2* XN;
+  double2* out;               // [B][n] final states (user layout)
+  int ntot;
 };
 
 // The next attempt's step: h capped at the time left (the final step lands
@@ -101,12 +106,16 @@ __global__ void k_batch_control(const __grid_constant__ ControlArgs a) {
   const ColState& c = a.c;
   if (q < a.ncol && lane == 0 && a.fx.on) {
     // fixed-step mode: accept every step whose norm is finite, t += dt as the
-    // reference's loop does, retire after nsteps steps
+    // reference's loop does, retire after nsteps steps.  The state stays
+    // unnormalised in XN with its norm in c.nrm (the next step's first
+    // product divides); the _pop entry and a finished pulse's final state are
+    // formed here, dividing as the reference's c /= ||c|| does.
+    c.retired[q] = 0;
     if (a.mode == 0) {
       c.h[q] = a.fx.dt;
       c.done[q] = (c.nsteps[q] <= 0) ? 1 : 0;
       c.accepted[q] = 0;
-      c.retired[q] = 0;
+      c.nrm[q] = 1.0;   // XN holds the normalised start state
       a.err[q] = 0ull;
       if (c.done[q]) retire(a, q);
       prepare_step(a, q);
@@ -123,8 +132,14 @@ __global__ void k_batch_control(const __grid_constant__ ControlArgs a) {
           c.nacc[q] += 1;
           c.accepted[q] = 1;
           c.nrm[q] = nrm;
-          if (a.fx.norm_hist)
-            a.fx.norm_hist[(long long)c.pulse_id[q] * a.fx.hist_ld + c.nacc[q] - 1] = nrm;
+          const long long id = c.pulse_id[q];
+          if (a.fx.norm_hist) a.fx.norm_hist[id * a.fx.hist_ld + c.nacc[q] - 1] = nrm;
+          if (a.fx.pop_hist) {
+            const double2 v = a.XN[(long long)a.fx.pop_index * a.ldc + q];
+            const double2 o = make_double2(v.x / nrm, v.y / nrm);
+            a.fx.pop_hist[id * a.fx.hist_ld + c.nacc[q]] =
+                __dadd_rn(__dmul_rn(o.x, o.x), __dmul_rn(o.y, o.y));
+          }
           if (c.nacc[q] >= c.nsteps[q]) c.done[q] = 1;
         } else {
           atomicOr(a.status, ST_NONFINITE);
@@ -186,6 +201,15 @@ __global__ void k_batch_control(const __grid_constant__ ControlArgs a) {
     }
   }
   __syncthreads();
+  if (a.fx.on && q < a.ncol && c.retired[q]) {
+    // fixed-step mode: the finished pulse's final state out, by its lanes
+    const double nrm = c.nrm[q];
+    const long long id = c.pulse_id[q];
+    for (int i = lane; i < a.ntot; i += kCtlLanes) {
+      const double2 v = a.XN[(long long)i * a.ldc + q];
+      a.out[id * a.ntot + i] = make_double2(v.x / nrm, v.y / nrm);
+    }
+  }
   if (q < a.ncol && lane < kNumStages) {
     // stage fields F(t + c_s h); in fixed-step mode F(t + dt) for every stage
     const double ts = a.fx.on ? c.t[q] + a.fx.dt : c.t[q] + c_C[lane] * c.hatt[q];
@@ -233,6 +257,18 @@ __global__ void k_batch_clear_retired(int* retired, int ncol) {
   pdl_wait();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q < ncol) retired[q] = 0;
+}
+
+// X = XN / nrm per column (fixed-step mode, before the resident tail takes
+// the batch over).
+__global__ void k_batch_normalize(double2* X, const double2* XN, const double* nrm, int ntot,
+                                  int ncol, int ldc) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)ntot * ncol) return;
+  const int i = (int)(e / ncol), q = (int)(e % ncol);
+  const long long idx = (long long)i * ldc + q;
+  const double2 v = XN[idx];
+  X[idx] = make_double2(v.x / nrm[q], v.y / nrm[q]);
 }
 
 // X columns in from the user layout [B][n].
@@ -378,6 +414,8 @@ StageArgs stage_args(mpc_ctx* c, int s, int ncol, double rtol, double atol, bool
   a.fs_stride = b->ldc;
   a.ws = b->ws;
   a.cnt = b->cnt;
+  a.nrm = b->c.nrm;
+  a.Xw = b->X;
   a.g = c->g;
   return a;
 }
@@ -441,6 +479,7 @@ int launch_horner_persistent(mpc_ctx* c, int ncol) {
 // lands in Y[0].
 int launch_horner(mpc_ctx* c, int p, int ncol) {
   StageArgs a = stage_args(c, p, ncol, 1.0, 1.0, false);
+  if (p == 0) a.Yin = c->batch->Y[0];   // the previous step's unnormalised x_new
   a.hg = rkf78::G[11 - p];
   a.vscale = (p == 0) ? rkf78::G[12] : 1.0;
   a.hlast = (p == 11) ? 1 : 0;
@@ -668,6 +707,17 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
   const int n = c->g.ntot;
   const int ldc = b->ldc;
 
+  // the fixed-step tuner times Horner steps on the work buffers (the first
+  // product writes X): it runs before the states are loaded, on unit norms
+  if (b->tile.empty() && !std::getenv("MPC_NO_AUTOTUNE") && (rc = autotune(c, B))) return rc;
+  if (fx.on && b->hplan.empty() && !c->no_persist && !c->force_persist &&
+      !std::getenv("MPC_NO_AUTOTUNE")) {
+    std::vector<double> ones(ldc, 1.0);
+    CK(cudaMemcpyAsync(s.nrm, ones.data(), sizeof(double) * ldc, cudaMemcpyHostToDevice,
+                       c->stream));
+    if ((rc = autotune_horner(c, B))) return rc;
+  }
+
   // per-column start state
   std::vector<int> ids(B);
   for (int i = 0; i < B; ++i) ids[i] = i;
@@ -685,6 +735,10 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
                      c->stream));
   k_batch_load<<<blocks_for((long long)n * B, 256), 256, 0, c->stream>>>(b->X, b->out, n, B, ldc);
   CK(cudaGetLastError());
+  // fixed-step mode: the state lives unnormalised in Y[0] (norm 1 at start)
+  if (fx.on)
+    CK(cudaMemcpyAsync(b->Y[0], b->X, sizeof(double2) * (size_t)n * ldc, cudaMemcpyDeviceToDevice,
+                       c->stream));
 
   ControlArgs ca{};
   ca.c = s;
@@ -699,6 +753,9 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
   ca.max_attempts = max_attempts > 0 ? max_attempts : 1000000000;
   ca.fx = fx;
   ca.status = c->d_status;
+  ca.XN = b->Y[0];
+  ca.out = b->out;
+  ca.ntot = n;
   ApplyArgs aa{};
   aa.X = b->X;
   aa.Xn = b->Y[1];
@@ -715,12 +772,16 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
   k_batch_control<<<blocks_for((long long)ncol * kCtlLanes, 128), 128, 0, c->stream>>>(ca);
   CK(cudaGetLastError());
   ca.mode = 1;
-  // pulses with nothing to do are retired by the start: write their states out
-  aa.ncol = ncol;
-  k_batch_apply<<<blocks_for((long long)n * ncol, 256), 256, 0, c->stream>>>(aa);
-  k_batch_clear_retired<<<blocks_for(ncol, 128), 128, 0, c->stream>>>(s.retired, ncol);
-  CK(cudaGetLastError());
-  c->launches += 3;
+  // pulses with nothing to do are retired by the start: write their states
+  // out (the control kernel itself does in fixed-step mode)
+  if (!fx.on) {
+    aa.ncol = ncol;
+    k_batch_apply<<<blocks_for((long long)n * ncol, 256), 256, 0, c->stream>>>(aa);
+    k_batch_clear_retired<<<blocks_for(ncol, 128), 128, 0, c->stream>>>(s.retired, ncol);
+    CK(cudaGetLastError());
+    c->launches += 2;
+  }
+  c->launches += 1;
 
   // Few pulses left on a system whose coupling fits on chip: the persistent
   // resident kernel takes over (unless the streamed path was asked for).
@@ -749,13 +810,22 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
   };
   // Compaction: the active columns move to the front of X and of every
   // per-column array (the results of retired pulses are already out).
+  // (in fixed-step mode the GEMM path keeps the state unnormalised in Y[0];
+  // the resident tail keeps it normalised in X)
+  bool state_in_y0 = fx.on;
   auto compact = [&](int act) -> int {
     CK(cudaMemcpyAsync(b->map, map_h.data(), sizeof(int) * act, cudaMemcpyHostToDevice,
                        c->stream));
     const int gb = blocks_for((long long)n * act, 256);
-    k_batch_gather_cols<<<gb, 256, 0, c->stream>>>(b->Y[0], b->X, b->map, n, act, ldc);
-    CK(cudaMemcpyAsync(b->X, b->Y[0], sizeof(double2) * (size_t)n * ldc,
-                       cudaMemcpyDeviceToDevice, c->stream));
+    if (state_in_y0) {  // the state is the unnormalised Y[0]; Y[1] is free between steps
+      k_batch_gather_cols<<<gb, 256, 0, c->stream>>>(b->Y[1], b->Y[0], b->map, n, act, ldc);
+      CK(cudaMemcpyAsync(b->Y[0], b->Y[1], sizeof(double2) * (size_t)n * ldc,
+                         cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+      k_batch_gather_cols<<<gb, 256, 0, c->stream>>>(b->Y[0], b->X, b->map, n, act, ldc);
+      CK(cudaMemcpyAsync(b->X, b->Y[0], sizeof(double2) * (size_t)n * ldc,
+                         cudaMemcpyDeviceToDevice, c->stream));
+    }
     const int sb = blocks_for(act, 128);
 #define GATHER(field, T)                                                                    \
   k_gather_scalar<T><<<sb, 128, 0, c->stream>>>(reinterpret_cast<T*>(b->scratch), s.field,  \
@@ -789,12 +859,6 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
     return MPC_OK;
   };
 
-  if (b->tile.empty() && !std::getenv("MPC_NO_AUTOTUNE") && (rc = autotune(c, B))) return rc;
-  if (fx.on && b->hplan.empty() && !c->no_persist && !c->force_persist &&
-      !std::getenv("MPC_NO_AUTOTUNE") &&
-      (rc = autotune_horner(c, B)))
-    return rc;
-
   // One attempted step of every active pulse: 13 stage GEMMs, the step
   // controller, the accepted-state update and the retirement flags.
   auto launch_attempt = [&]() -> int {
@@ -814,6 +878,8 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
       CK(mpc_launch_pdl(k_batch_control, dim3(blocks_for((long long)ncol * kCtlLanes, 128)),
                         dim3(128), 0, c->stream, ca));
     }
+    c->launches += 1;
+    if (fx.on) return MPC_OK;  // renormalisation in the next step's first product
     {
       ProfScope ps(c, MPC_KERNEL_BATCH_OTHER);
       CK(mpc_launch_pdl(k_batch_apply, dim3(blocks_for((long long)n * ncol, 256)), dim3(256), 0,
@@ -824,7 +890,7 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
       CK(mpc_launch_pdl(k_batch_clear_retired, dim3(blocks_for(ncol, 128)), dim3(128), 0,
                         c->stream, s.retired, ncol));
     }
-    c->launches += 3;
+    c->launches += 2;
     return MPC_OK;
   };
   // Attempts run in groups of check_every between reads of the done flags;
@@ -861,7 +927,7 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
     }
     if (use_graph) {
       CK(cudaGraphLaunch(gexec, c->stream));
-      c->launches += (fx.on ? (horner_persistent(c, ncol) ? 4LL : 15LL) : 16LL) * check_every;
+      c->launches += (fx.on ? (horner_persistent(c, ncol) ? 2LL : 13LL) : 16LL) * check_every;
       return MPC_OK;
     }
     for (int k = 0; k < check_every; ++k)
@@ -875,6 +941,13 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
     if (act == 0) break;
     if (pres && act <= pres) {
       if (act < ncol && (rc = compact(act))) break;
+      if (fx.on) {  // the resident kernel takes normalised states in X
+        k_batch_normalize<<<blocks_for((long long)n * ncol, 256), 256, 0, c->stream>>>(
+            b->X, b->Y[0], s.nrm, n, ncol, ldc);
+        CK(cudaGetLastError());
+        ++c->launches;
+        state_in_y0 = false;
+      }
       BatchResLaunch l{};
       l.c = s;
       l.res = b->res;

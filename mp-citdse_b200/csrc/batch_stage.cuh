@@ -113,6 +113,11 @@ struct StageArgs {
   double hg;
   double vscale;
   int hlast;
+  // the first product takes the previous step's unnormalised x_new (Yin) and
+  // its norm per pulse (nrm), forms x = x_new / ||x_new|| on the fly and
+  // stores it (Xw) for the step's later products
+  const double* nrm;
+  double2* Xw;
   // adjoint stages (MODE 1): Yin = kbar_s, K = ybar slabs, Yout = kbar_{s-1}
   // (or lambda_n after stage 0)
   const double2* Ys;     // the forward stage input y_s
@@ -502,10 +507,25 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const ProdSel& ps
           if (!qv || r >= nL) continue;
           const long long i = g.state_off[L] + r;
           const long long idx = i * a.ldc + q;
-          const double wre = vs * acc[mt][nt][2 * hr], wim = vs * acc[mt][nt][2 * hr + 1];
-          const double2 v0 = ps.Yin[idx];
-          const double2 v = make_double2(vs * v0.x, vs * v0.y);
-          const double2 x = a.X[idx];
+          double wre, wim;
+          double2 v, x;
+          if (ps.stage == 0) {
+            // x = x_new / ||x_new|| (the reference's c /= ||c||), its coupling
+            // D x = (D x_new) / ||x_new||
+            const double nq = a.nrm[q];
+            const double2 z = ps.Yin[idx];
+            x = make_double2(z.x / nq, z.y / nq);
+            a.Xw[idx] = x;
+            wre = vs * (acc[mt][nt][2 * hr] / nq);
+            wim = vs * (acc[mt][nt][2 * hr + 1] / nq);
+            v = make_double2(vs * x.x, vs * x.y);
+          } else {
+            wre = vs * acc[mt][nt][2 * hr];
+            wim = vs * acc[mt][nt][2 * hr + 1];
+            const double2 v0 = ps.Yin[idx];
+            v = make_double2(vs * v0.x, vs * v0.y);
+            x = a.X[idx];
+          }
           const double e = a.eps[i];
           double kre, kim;  // M(F) v, formed as the stage form forms k
           if (a.gauge == 0) {
@@ -845,7 +865,7 @@ __global__ void __launch_bounds__(BTHREADS, 2) k_batch_horner(const __grid_const
     if (s_dead) break;
     ProdSel ps;
     ps.stage = p;
-    ps.Yin = (p == 0) ? h.a.X : h.Y[p & 1];
+    ps.Yin = h.Y[p & 1];   // p = 0: the previous step's unnormalised x_new in Y[0]
     ps.Yout = const_cast<double2*>(h.Y[(p + 1) & 1]);
     ps.hg = c_G[11 - p];
     ps.vscale = (p == 0) ? c_G[12] : 1.0;
