@@ -299,6 +299,7 @@ struct mpc_adjoint_state {
   std::vector<void*> allocs;
   bool have_forward = false;
   bool resident = false;      // both passes on the shared-memory-resident kernels
+  bool last_kept = false;     // the streamed forward kept the last segment's states
 };
 
 namespace {
@@ -432,14 +433,31 @@ int mpc_objective(mpc_ctx* c, const mpc_pulse* p, int K, const double* u, double
                                       (long long)n)))
       return rc;
   } else {
-    for (int st = 0; st < steps; ++st) {
-      double2* xn = ((st + 1) % ckpt_every == 0 || st + 1 == steps)
-                        ? a->ckpts + n * ((st + 1 + ckpt_every - 1) / ckpt_every)
+    // the last segment keeps every state, stage input and norm as the reverse
+    // pass's recompute would, so the reverse pass starts sweeping at once
+    const int n0_last = (a->nseg - 1) * ckpt_every;
+    for (int st = 0; st < n0_last; ++st) {
+      double2* xn = ((st + 1) % ckpt_every == 0)
+                        ? a->ckpts + n * ((st + 1) / ckpt_every)
                         : a->segX + n * ((st & 1) ? 0 : 1);
       if ((rc = fwd_step(c, st, dt, x, ys, xn, a->segN))) return rc;
       x = xn;
     }
+    CK(cudaMemcpyAsync(a->segX, a->ckpts + n * (a->nseg - 1), sizeof(double2) * n,
+                       cudaMemcpyDeviceToDevice, c->stream));
+    for (int j = 0; j < steps - n0_last; ++j) {
+      double2* yj[14];
+      yj[0] = nullptr;
+      for (int s = 1; s < kNumStages; ++s) yj[s] = a->segY + n * ((size_t)j * kNumStages + s);
+      yj[13] = a->segY + n * ((size_t)j * kNumStages);  // slot 0 holds x_new (y_0 = x_n)
+      if ((rc = fwd_step(c, n0_last + j, dt, a->segX + n * j, yj, a->segX + n * (j + 1),
+                         a->segN + j)))
+        return rc;
+    }
+    CK(cudaMemcpyAsync(a->ckpts + n * a->nseg, a->segX + n * (steps - n0_last),
+                       sizeof(double2) * n, cudaMemcpyDeviceToDevice, c->stream));
   }
+  a->last_kept = !a->resident;
   // objective on the host from x_N
   std::vector<double> xN(2 * c->g.ntot), eps(c->g.ntot);
   CK(cudaMemcpyAsync(xN.data(), a->ckpts + n * a->nseg, nb, cudaMemcpyDeviceToHost, c->stream));
@@ -530,10 +548,13 @@ int mpc_objective_backward(mpc_ctx* c, double* grad_u, double* dJdF) {
         return rc;
       continue;
     }
-    // recompute the segment, keeping states, stage inputs and norms
-    CK(cudaMemcpyAsync(a->segX, a->ckpts + n * seg, sizeof(double2) * n, cudaMemcpyDeviceToDevice,
-                       c->stream));
-    for (int j = 0; j < len; ++j) {
+    // recompute the segment, keeping states, stage inputs and norms (the
+    // forward kept the last one)
+    const bool kept = a->last_kept && seg == nseg - 1;
+    if (!kept)
+      CK(cudaMemcpyAsync(a->segX, a->ckpts + n * seg, sizeof(double2) * n,
+                         cudaMemcpyDeviceToDevice, c->stream));
+    for (int j = 0; j < len && !kept; ++j) {
       double2* ys[14];
       ys[0] = nullptr;
       for (int s = 1; s < kNumStages; ++s) ys[s] = a->segY + n * ((size_t)j * kNumStages + s);
@@ -565,6 +586,7 @@ int mpc_objective_backward(mpc_ctx* c, double* grad_u, double* dJdF) {
                         c->combine_grid, a->fbar + stp));
     }
   }
+  a->last_kept = false;  // the sweep overwrote the kept segment: a repeat recomputes it
   std::vector<double> fb(steps);
   CK(cudaMemcpyAsync(fb.data(), a->fbar, sizeof(double) * steps, cudaMemcpyDeviceToHost,
                      c->stream));
