@@ -788,6 +788,13 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
   const int pres = (c->path == MPC_PATH_STREAMING) ? 0 : mpc_batch_res_pmax(c);
 
   std::vector<int> done_h(B), map_h(B);
+  // fixed-step mode: every active pulse takes one step per attempt, so the
+  // host knows when the next one finishes -- the attempts up to then run
+  // without reading the done flags in between
+  std::vector<int> colpid(B), steps_h(nsteps ? nsteps : zeros.data(),
+                                      (nsteps ? nsteps : zeros.data()) + B);
+  for (int q = 0; q < B; ++q) colpid[q] = q;
+  long long steps_done = 0;
   auto width = [](int nc) {
     return 2 * nc <= 16 ? 16 : (2 * nc <= 128 ? (2 * nc + 31) / 32 * 32 : (2 * nc + 63) / 64 * 64);
   };
@@ -846,6 +853,11 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
     GATHER(nrm, double)
     GATHER(retired, int)
     GATHER(nsteps, int)
+    {
+      std::vector<int> cp(act);
+      for (int k = 0; k < act; ++k) cp[k] = colpid[map_h[k]];
+      std::copy(cp.begin(), cp.end(), colpid.begin());
+    }
     for (int st = 0; st < kNumStages; ++st) {
       k_gather_scalar<double><<<sb, 128, 0, c->stream>>>(reinterpret_cast<double*>(b->scratch),
                                                          b->Fs + st * ldc, b->map, act);
@@ -975,6 +987,23 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
     }
     // compact when the GEMM can drop a column tile or use a narrower one
     if (width(act) < width(ncol) && (rc = compact(act))) break;
+    if (fx.on) {
+      // run up to the next pulse's last step: whole graph groups, then single
+      // attempts, then look at the done flags again
+      long long until = -1;   // a finished pulse has no steps left
+      for (int q = 0; q < ncol; ++q) {
+        const long long left = (long long)steps_h[colpid[q]] - steps_done;
+        if (left > 0 && (until < 0 || left < until)) until = left;
+      }
+      if (until <= 0) until = 1;
+      for (long long k = 0; k + check_every <= until && rc == MPC_OK; k += check_every)
+        rc = run_group();
+      for (long long k = until - until % check_every; k < until && rc == MPC_OK; ++k)
+        rc = launch_attempt();
+      if (rc) break;
+      steps_done += until;
+      continue;
+    }
     if ((rc = run_group())) break;
   }
   drop_graph();
