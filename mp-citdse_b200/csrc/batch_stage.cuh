@@ -141,19 +141,19 @@ struct StageArgs {
 // last chunk of a block is zero fill) and only this warp's first mt_lim
 // 16-row m-tiles hold rows of the block: the rest would add exact zeros or
 // rows that are never stored, so they are skipped (warp-uniform branches).
-template <int BN, bool IS_P>
-__device__ __forceinline__ void chunk_mma(const double* As, const double* Bs, int wm, int wn,
+template <int BN, bool IS_P, bool FULL>
+__device__ __forceinline__ void chunk_mma_body(const double* As, const double* Bs, int wm, int wn,
                                           int gq, int tq, int nks, int mt_lim,
                                           double (&acc)[Tile<BN>::WMT][Tile<BN>::WNT][4]) {
   constexpr int WMT = Tile<BN>::WMT, WNT = Tile<BN>::WNT;
   constexpr int LDB = BN + 4;
 #pragma unroll
   for (int ks = 0; ks < BK / 8; ++ks) {
-    if (ks >= nks) break;
+    if (!FULL && ks >= nks) break;
     double af[WMT][4], bf[WNT][2];
 #pragma unroll
     for (int mt = 0; mt < WMT; ++mt) {
-      if (mt >= mt_lim) break;
+      if (!FULL && mt >= mt_lim) break;
       const int m = wm * (WMT * 16) + mt * 16 + gq;
       const int k = ks * 8 + tq;
       if constexpr (IS_P) {
@@ -177,11 +177,23 @@ __device__ __forceinline__ void chunk_mma(const double* As, const double* Bs, in
     }
 #pragma unroll
     for (int mt = 0; mt < WMT; ++mt) {
-      if (mt >= mt_lim) break;
+      if (!FULL && mt >= mt_lim) break;
 #pragma unroll
       for (int nt = 0; nt < WNT; ++nt) dmma16x8x8(acc[mt][nt], af[mt], bf[nt]);
     }
   }
+}
+
+// A whole chunk on a warp whose m-tiles all hold rows (the usual case) runs
+// without the skip branches, so its fragment loads schedule ahead of the DMMAs.
+template <int BN, bool IS_P>
+__device__ __forceinline__ void chunk_mma(const double* As, const double* Bs, int wm, int wn,
+                                          int gq, int tq, int nks, int mt_lim,
+                                          double (&acc)[Tile<BN>::WMT][Tile<BN>::WNT][4]) {
+  if (nks == BK / 8 && mt_lim == Tile<BN>::WMT)
+    chunk_mma_body<BN, IS_P, true>(As, Bs, wm, wn, gq, tq, nks, mt_lim, acc);
+  else
+    chunk_mma_body<BN, IS_P, false>(As, Bs, wm, wn, gq, tq, nks, mt_lim, acc);
 }
 
 // One output tile of a stage (or Horner product): tile index `bid` (the
@@ -205,8 +217,8 @@ __device__ __forceinline__ ProdSel prod_sel(const StageArgs& a) {
 // P product goes into accP and the Q product into accQ, so each warp keeps
 // twice as many independent DMMA accumulations in flight as with one chunk
 // at a time, with each accumulator's terms in the same order as before.
-template <int BN>
-__device__ __forceinline__ void pair_mma(const double* AsP, const double* BsP, const double* AsQ,
+template <int BN, bool FULL>
+__device__ __forceinline__ void pair_mma_body(const double* AsP, const double* BsP, const double* AsQ,
                                          const double* BsQ, int wm, int wn, int gq, int tq,
                                          int nksP, int nksQ, int mt_lim,
                                          double (&accP)[Tile<BN>::WMT][Tile<BN>::WNT][4],
@@ -216,11 +228,11 @@ __device__ __forceinline__ void pair_mma(const double* AsP, const double* BsP, c
 #pragma unroll
   for (int ks = 0; ks < BK / 8; ++ks) {
     const int k = ks * 8 + tq;
-    if (ks < nksP) {
+    if (FULL || ks < nksP) {
       double af[WMT][4], bf[WNT][2];
 #pragma unroll
       for (int mt = 0; mt < WMT; ++mt) {
-        if (mt >= mt_lim) break;
+        if (!FULL && mt >= mt_lim) break;
         const int m = wm * (WMT * 16) + mt * 16 + gq;
         af[mt][0] = AsP[k * LDA_P + m];
         af[mt][1] = AsP[k * LDA_P + m + 8];
@@ -235,16 +247,16 @@ __device__ __forceinline__ void pair_mma(const double* AsP, const double* BsP, c
       }
 #pragma unroll
       for (int mt = 0; mt < WMT; ++mt) {
-        if (mt >= mt_lim) break;
+        if (!FULL && mt >= mt_lim) break;
 #pragma unroll
         for (int nt = 0; nt < WNT; ++nt) dmma16x8x8(accP[mt][nt], af[mt], bf[nt]);
       }
     }
-    if (ks < nksQ) {
+    if (FULL || ks < nksQ) {
       double af[WMT][4], bf[WNT][2];
 #pragma unroll
       for (int mt = 0; mt < WMT; ++mt) {
-        if (mt >= mt_lim) break;
+        if (!FULL && mt >= mt_lim) break;
         const int m = wm * (WMT * 16) + mt * 16 + gq;
         af[mt][0] = AsQ[m * LDA_Q + k];
         af[mt][1] = AsQ[(m + 8) * LDA_Q + k];
@@ -259,12 +271,24 @@ __device__ __forceinline__ void pair_mma(const double* AsP, const double* BsP, c
       }
 #pragma unroll
       for (int mt = 0; mt < WMT; ++mt) {
-        if (mt >= mt_lim) break;
+        if (!FULL && mt >= mt_lim) break;
 #pragma unroll
         for (int nt = 0; nt < WNT; ++nt) dmma16x8x8(accQ[mt][nt], af[mt], bf[nt]);
       }
     }
   }
+}
+
+template <int BN>
+__device__ __forceinline__ void pair_mma(const double* AsP, const double* BsP, const double* AsQ,
+                                         const double* BsQ, int wm, int wn, int gq, int tq,
+                                         int nksP, int nksQ, int mt_lim,
+                                         double (&accP)[Tile<BN>::WMT][Tile<BN>::WNT][4],
+                                         double (&accQ)[Tile<BN>::WMT][Tile<BN>::WNT][4]) {
+  if (nksP == BK / 8 && nksQ == BK / 8 && mt_lim == Tile<BN>::WMT)
+    pair_mma_body<BN, true>(AsP, BsP, AsQ, BsQ, wm, wn, gq, tq, nksP, nksQ, mt_lim, accP, accQ);
+  else
+    pair_mma_body<BN, false>(AsP, BsP, AsQ, BsQ, wm, wn, gq, tq, nksP, nksQ, mt_lim, accP, accQ);
 }
 
 template <int BN, int NSTB, int MODE, int SPLIT>
