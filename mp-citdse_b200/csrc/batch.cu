@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "batch_stage.cuh"
+#include "batch_tma.cuh"
 #include "batch_types.h"
 #include "ctx.h"
 #include "dev_util.cuh"
@@ -327,11 +328,19 @@ struct mpc_batch_state {
   std::vector<int> tile;
   std::vector<double> tile_us;
   // fixed-step steps, per width bucket: -1 one launch per Horner product
-  // (with the tuned variant), v >= 0 the persistent launch on variant v;
+  // (with the tuned variant), v >= 0 the persistent launch on variant v,
+  // kPlanTma + s one TMA-fed launch per product on TMA shape s;
   // microseconds per step of the choice
   std::vector<int> hplan;
   std::vector<double> hplan_us;
+  // TMA tensor maps of the TMA-fed Horner products (device copy)
+  CUtensorMap* d_maps = nullptr;
+  bool tma_ok = false;
 };
+
+namespace {
+constexpr int kPlanTma = 100;
+}
 
 namespace {
 
@@ -382,6 +391,37 @@ int ensure_batch(mpc_ctx* c, int B) {
       (rc = balloc(b, &b->res.nacc, ldc)) || (rc = balloc(b, &b->res.nrej, ldc)) ||
       (rc = balloc(b, &b->res.t, ldc)) || (rc = balloc(b, &b->res.status, ldc)))
     return rc;
+  // tensor maps of the TMA-fed Horner products: the coupling blocks in both
+  // box shapes and the two product buffers (the library's pitches and
+  // allocations satisfy TMA's 16-byte rules)
+  {
+    static bool attrs_set[64] = {};
+    if (c->device >= 0 && c->device < 64 && !attrs_set[c->device]) {
+      CK(set_tma_attrs());
+      attrs_set[c->device] = true;
+    }
+    const int nblk = g.nblk;
+    std::vector<CUtensorMap> maps(2 * (size_t)nblk + 2);
+    bool ok = nblk >= 1;
+    for (int L = 0; ok && L < nblk; ++L) {
+      const BlockGeom& bg = g.blk[L];
+      const double* base = c->d_D + bg.d_off;
+      ok = mpc_encode_map_2d(&maps[L], base, bg.ncol, bg.nrow, 8ull * bg.pitch, 16, BK, true) ==
+               MPC_OK &&
+           mpc_encode_map_2d(&maps[nblk + L], base, bg.ncol, bg.nrow, 8ull * bg.pitch, 16, BM,
+                             true) == MPC_OK;
+    }
+    for (int i = 0; ok && i < 2; ++i)
+      ok = mpc_encode_map_2d(&maps[2 * nblk + i], b->Y[i], 2ull * ldc, g.ntot, 16ull * ldc, 16,
+                             BK, true) == MPC_OK;
+    if (ok) {
+      if ((rc = balloc(b, reinterpret_cast<char**>(&b->d_maps), sizeof(CUtensorMap) * maps.size())))
+        return rc;
+      CK(cudaMemcpy(b->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(),
+                    cudaMemcpyHostToDevice));
+    }
+    b->tma_ok = ok;
+  }
   CK(cudaMemsetAsync(b->X, 0, nel * sizeof(double2), c->stream));
   CK(cudaMemsetAsync(b->cnt, 0, split_cnt_ints(nrt, ldc) * sizeof(int), c->stream));
   CK(cudaMemsetAsync(b->Y[0], 0, nel * sizeof(double2), c->stream));
@@ -434,6 +474,7 @@ int launch_stage(mpc_ctx* c, const StageArgs& a) {
 int horner_plan(mpc_ctx* c, int ncol) {
   if (c->no_persist) return -1;
   const mpc_batch_state* b = c->batch;
+  if (c->force_tma > 0 && b->tma_ok) return kPlanTma + std::min(c->force_tma - 1, kNumTmaShapes - 1);
   if (c->force_persist) return mpc_batch_variant(c, ncol);
   const int j = width_bucket(ncol);
   if (j < (int)b->hplan.size()) return b->hplan[j];
@@ -443,7 +484,6 @@ int horner_plan(mpc_ctx* c, int ncol) {
   return (long long)ncolt * b->nrowtiles >= c->num_sms ? v : -1;
 }
 
-bool horner_persistent(mpc_ctx* c, int ncol) { return horner_plan(c, ncol) >= 0; }
 
 int launch_horner_persistent_v(mpc_ctx* c, int ncol, int v) {
   mpc_batch_state* b = c->batch;
@@ -468,9 +508,6 @@ int launch_horner_persistent_v(mpc_ctx* c, int ncol, int v) {
   return MPC_OK;
 }
 
-int launch_horner_persistent(mpc_ctx* c, int ncol) {
-  return launch_horner_persistent_v(c, ncol, horner_plan(c, ncol));
-}
 
 // Product p = 0 .. 11 of a fixed-step (frozen-field) step evaluated as the
 // stability polynomial by Horner's rule: v_12 = G[12] x, then
@@ -487,6 +524,49 @@ int launch_horner(mpc_ctx* c, int p, int ncol) {
   ++c->launches;
   CK(launch_variant<2>(c->stream, mpc_batch_variant(c, a.ncol), a));
   return MPC_OK;
+}
+
+// Product p of a fixed step as the TMA-fed launch on TMA tile shape `shape`.
+int launch_horner_tma(mpc_ctx* c, int p, int ncol, int shape) {
+  mpc_batch_state* b = c->batch;
+  HornerTmaArgs h{};
+  h.a = stage_args(c, p, ncol, 1.0, 1.0, false);
+  h.maps = b->d_maps;
+  h.Y[0] = b->Y[0];
+  h.Y[1] = b->Y[1];
+  h.status = c->d_status;
+  h.wait_ns = c->wait_limit_ns;
+  const int bn = kTmaShapes[shape].bn;
+  h.ncolt = (2 * ncol + bn - 1) / bn;
+  h.p = p;
+  ProfScope ps(c, MPC_KERNEL_BATCH_STAGE);
+  ++c->launches;
+  CK(launch_horner_tma_shape(c->stream, shape, h, c->num_sms));
+  return MPC_OK;
+}
+
+// The 12 products of one fixed step of ncol pulses, run as plan says.
+int launch_horner_plan(mpc_ctx* c, int ncol, int plan) {
+  int rc;
+  if (plan >= kPlanTma) {
+    for (int p = 0; p < 12; ++p)
+      if ((rc = launch_horner_tma(c, p, ncol, plan - kPlanTma))) return rc;
+    return MPC_OK;
+  }
+  if (plan >= 0) return launch_horner_persistent_v(c, ncol, plan);
+  for (int p = 0; p < 12; ++p)
+    if ((rc = launch_horner(c, p, ncol))) return rc;
+  return MPC_OK;
+}
+
+int launch_horner_step(mpc_ctx* c, int ncol) {
+  return launch_horner_plan(c, ncol, horner_plan(c, ncol));
+}
+
+// Kernel launches of one fixed step (its products and the controller).
+long long horner_step_launches(mpc_ctx* c, int ncol) {
+  const int plan = horner_plan(c, ncol);
+  return (plan >= 0 && plan < kPlanTma) ? 2 : 13;
 }
 
 // Times every variant on a single right-hand side (stage 0, k only) at
@@ -550,23 +630,16 @@ int autotune_horner(mpc_ctx* c, int max_cols) {
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  const int cands[] = {-1, 0, 1, 2, 3, 4};
+  std::vector<int> cands = {-1, 0, 1, 2, 3, 4};
+  if (b->tma_ok && !c->no_tma)
+    for (int sh = 0; sh < kNumTmaShapes; ++sh) cands.push_back(kPlanTma + sh);
   int rc = MPC_OK;
   const long long l0 = c->launches;
   for (int j = 0; j <= top && rc == MPC_OK; ++j) {
     const int w = std::min(1 << j, b->ldc);
     double best = 1e300;
     for (int v : cands) {
-      auto step = [&]() -> int {
-        if (v < 0) {
-          for (int p = 0; p < 12; ++p) {
-            int r = launch_horner(c, p, w);
-            if (r) return r;
-          }
-          return MPC_OK;
-        }
-        return launch_horner_persistent_v(c, w, v);
-      };
+      auto step = [&]() -> int { return launch_horner_plan(c, w, v); };
       for (int r = 0; r < 2 && rc == MPC_OK; ++r) rc = step();
       if (rc) break;
       CK(cudaEventRecord(e0, c->stream));
@@ -660,11 +733,17 @@ int mpc_batch_fixed_plan(mpc_ctx* c, double* table, int cap) {
   const int rows = (int)b->hplan.size();
   for (int j = 0; table && j < rows && j < cap; ++j) {
     const int v = b->hplan[j];
-    const int vv = v >= 0 ? v : mpc_batch_variant(c, std::min(1 << j, b->ldc));
     table[5 * j + 0] = std::min(1 << j, b->ldc);
-    table[5 * j + 1] = v >= 0 ? 1 : 0;
-    table[5 * j + 2] = kVariants[vv].bn;
-    table[5 * j + 3] = v >= 0 ? (kVariants[vv].nst >= 6 ? 3 : 2) : kVariants[vv].nst;
+    if (v >= kPlanTma) {
+      table[5 * j + 1] = 2;
+      table[5 * j + 2] = kTmaShapes[v - kPlanTma].bn;
+      table[5 * j + 3] = kTmaShapes[v - kPlanTma].ns;
+    } else {
+      const int vv = v >= 0 ? v : mpc_batch_variant(c, std::min(1 << j, b->ldc));
+      table[5 * j + 1] = v >= 0 ? 1 : 0;
+      table[5 * j + 2] = kVariants[vv].bn;
+      table[5 * j + 3] = v >= 0 ? (kVariants[vv].nst >= 6 ? 3 : 2) : kVariants[vv].nst;
+    }
     table[5 * j + 4] = b->hplan_us[j];
   }
   return rows;
@@ -707,10 +786,12 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
   const int n = c->g.ntot;
   const int ldc = b->ldc;
 
+  if (fx.on && c->force_tma > 0 && !b->tma_ok)
+    return mpc_fail(MPC_ERR_CUDA, "MPC_FORCE_TMA: the TMA tensor maps could not be set up");
   // the fixed-step tuner times Horner steps on the work buffers (the first
   // product writes X): it runs before the states are loaded, on unit norms
   if (b->tile.empty() && !std::getenv("MPC_NO_AUTOTUNE") && (rc = autotune(c, B))) return rc;
-  if (fx.on && b->hplan.empty() && !c->no_persist && !c->force_persist &&
+  if (fx.on && b->hplan.empty() && !c->no_persist && !c->force_persist && !c->force_tma &&
       !std::getenv("MPC_NO_AUTOTUNE")) {
     std::vector<double> ones(ldc, 1.0);
     CK(cudaMemcpyAsync(s.nrm, ones.data(), sizeof(double) * ldc, cudaMemcpyHostToDevice,
@@ -874,11 +955,8 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
   // One attempted step of every active pulse: 13 stage GEMMs, the step
   // controller, the accepted-state update and the retirement flags.
   auto launch_attempt = [&]() -> int {
-    if (fx.on && horner_persistent(c, ncol)) {  // frozen field, one persistent launch
-      if ((rc = launch_horner_persistent(c, ncol))) return rc;
-    } else if (fx.on) {  // frozen field: 12 products of the stability polynomial
-      for (int p = 0; p < 12; ++p)
-        if ((rc = launch_horner(c, p, ncol))) return rc;
+    if (fx.on) {  // frozen field: the 12 products of the stability polynomial
+      if ((rc = launch_horner_step(c, ncol))) return rc;
     } else {
       for (int st = 0; st < kNumStages; ++st)
         if ((rc = launch_stage(c, stage_args(c, st, ncol, rtol, atol, false)))) return rc;
@@ -939,7 +1017,7 @@ int batch_run(mpc_ctx* c, int B, const mpc_pulse* pulses, const double* t0, cons
     }
     if (use_graph) {
       CK(cudaGraphLaunch(gexec, c->stream));
-      c->launches += (fx.on ? (horner_persistent(c, ncol) ? 2LL : 13LL) : 16LL) * check_every;
+      c->launches += (fx.on ? horner_step_launches(c, ncol) : 16LL) * check_every;
       return MPC_OK;
     }
     for (int k = 0; k < check_every; ++k)

@@ -17,6 +17,10 @@
 // Records `fmt` as the calling thread's last error and returns `code`.
 int mpc_fail(int code, const char* fmt, ...);
 int mpc_internal_fail(int code, const char* msg);
+// A 2-D FP64 tensor map for TMA loads (mpc_tdse.cu).
+int mpc_encode_map_2d(CUtensorMap* m, const void* base, unsigned long long inner,
+                      unsigned long long outer, unsigned long long row_bytes, unsigned box_inner,
+                      unsigned box_outer, bool swizzle128);
 
 #define CK(call)                                                                         \
   do {                                                                                   \
@@ -83,6 +87,11 @@ struct mpc_ctx {
   // MPC_FORCE_PERSIST=1 at context creation: the persistent launch at every
   // width (tests of that path; it is correct at any width, not always faster)
   bool force_persist = false;
+  // MPC_FORCE_TMA=s at context creation: the batched fixed step as the
+  // TMA-fed product launches on TMA tile shape s - 1 at every width (tests);
+  // MPC_NO_TMA=1: the fixed-step tuner leaves the TMA-fed launches out
+  int force_tma = 0;
+  bool no_tma = false;
   // grid-barrier wait limit of the persistent kernels (mpc_ctx_set_wait_limit)
   unsigned long long wait_limit_ns = 2000000000ull;
   // the next persistent launch gets an unreachable barrier target

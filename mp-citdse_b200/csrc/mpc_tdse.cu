@@ -71,6 +71,31 @@ int get_encode(EncodeTiledFn* fn) {
   return MPC_OK;
 }
 
+}  // namespace
+
+// A 2-D FP64 tensor map for TMA loads of [outer][inner] elements, rows
+// row_bytes apart, boxes of box_inner x box_outer; swizzle128: the 128-byte
+// swizzle (box_inner * 8 must then be 128).
+int mpc_encode_map_2d(CUtensorMap* m, const void* base, unsigned long long inner,
+                      unsigned long long outer, unsigned long long row_bytes, unsigned box_inner,
+                      unsigned box_outer, bool swizzle128) {
+  EncodeTiledFn enc = nullptr;
+  int rc;
+  if ((rc = get_encode(&enc))) return rc;
+  cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+  cuuint64_t strides[1] = {(cuuint64_t)row_bytes};
+  cuuint32_t box[2] = {(cuuint32_t)box_inner, (cuuint32_t)box_outer};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(base), dims, strides,
+                   box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(MPC_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return MPC_OK;
+}
+
+namespace {
+
 template <class T>
 int dalloc(mpc_ctx* c, T** p, size_t count) {
   void* q = nullptr;
@@ -495,6 +520,8 @@ int mpc_ctx_create(int L_max, const int* state_sz, const double* eig, const doub
   if (const char* v = std::getenv("MPC_BATCH_VARIANT")) c->forced_variant = std::atoi(v);
   c->no_persist = std::getenv("MPC_NO_PERSIST") != nullptr;
   c->force_persist = std::getenv("MPC_FORCE_PERSIST") != nullptr;
+  if (const char* ft = std::getenv("MPC_FORCE_TMA")) c->force_tma = std::max(0, std::atoi(ft));
+  c->no_tma = std::getenv("MPC_NO_TMA") != nullptr;
   c->gauge = gauge;
   c->n.assign(state_sz, state_sz + L_max + 1);
   CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));

@@ -206,3 +206,42 @@ def test_persistent_step_equals_one_launch_per_product(monkeypatch):
     # entries past a pulse's own step count are unset (NaN) in both
     assert np.array_equal(p1, p2, equal_nan=True)
     assert np.array_equal(n1, n2, equal_nan=True)
+
+
+@pytest.mark.parametrize("shape", [1, 2])
+@pytest.mark.parametrize("system", ["uneven_v", "h1e"])
+def test_tma_step_equals_cp_async_step(monkeypatch, shape, system):
+    """The TMA-fed product launches (swizzled tiles read through permuted
+    fragment rows and columns) against the cp.async launches: the same sums
+    in the same order, so the same bits -- final states, _pop columns and
+    pre-renormalisation norms -- through retirements and compaction."""
+    from mpc_tdse.structure1e import hydrogen
+    from mpc_tdse.systems import random_system
+
+    if system == "h1e":
+        s = hydrogen(n=300, k=9, R=200.0, l_max=5, gauge="l", states=[292] * 6)
+        B, gauge = 80, "l"
+    else:
+        # four blocks of uneven sizes (partial row tiles and k chunks), velocity gauge
+        s = random_system([60, 70, 50, 90], gauge="v", seed=8, e_max=6.0)
+        B, gauge = 40, "v"
+    Io, w = mpc_tdse.to_au(2e14, 1.5498)
+    tau = mpc_tdse.period(w, 1)
+    ps = [mpc_tdse.pulse_setup("sine", gauge, Io * (0.5 + 0.01 * b), w, 0.0, 1, tau)
+          for b in range(B)]
+    X0 = np.zeros((B, s.ntot), complex)
+    X0[:, 0] = 1.0
+    steps = [40 + 5 * (b % 11) for b in range(B)]
+    out = []
+    for env in ("MPC_NO_PERSIST", "MPC_FORCE_TMA"):
+        monkeypatch.delenv("MPC_NO_PERSIST", raising=False)
+        monkeypatch.delenv("MPC_FORCE_TMA", raising=False)
+        monkeypatch.setenv(env, "1" if env == "MPC_NO_PERSIST" else str(shape))
+        with mpc_tdse.Context.from_system(s) as ctx:
+            ctx.set_path("streaming")
+            # (MPC_FORCE_TMA fails the call if the TMA launch cannot be set up)
+            out.append(ctx.batch_advance(ps, 0.0, 0.05, steps, X0, history=True))
+    (X1, p1, n1), (X2, p2, n2) = out
+    assert np.array_equal(X1, X2)
+    assert np.array_equal(p1, p2, equal_nan=True)
+    assert np.array_equal(n1, n2, equal_nan=True)
