@@ -333,8 +333,9 @@ struct mpc_batch_state {
   // microseconds per step of the choice
   std::vector<int> hplan;
   std::vector<double> hplan_us;
-  // TMA tensor maps of the TMA-fed Horner products (device copy)
-  CUtensorMap* d_maps = nullptr;
+  // TMA tensor maps of the TMA-fed Horner products
+  std::vector<CUtensorMap> maps;
+  CUtensorMap ymaps[kNumTmaShapes][2];
   bool tma_ok = false;
 };
 
@@ -401,25 +402,22 @@ int ensure_batch(mpc_ctx* c, int B) {
       attrs_set[c->device] = true;
     }
     const int nblk = g.nblk;
-    std::vector<CUtensorMap> maps(2 * (size_t)nblk + 2);
-    bool ok = nblk >= 1;
+    std::vector<CUtensorMap>& maps = b->maps;
+    maps.assign(2 * kTmaMaxBlocks, CUtensorMap{});
+    bool ok = nblk >= 1 && nblk <= kTmaMaxBlocks;
     for (int L = 0; ok && L < nblk; ++L) {
       const BlockGeom& bg = g.blk[L];
       const double* base = c->d_D + bg.d_off;
-      ok = mpc_encode_map_2d(&maps[L], base, bg.ncol, bg.nrow, 8ull * bg.pitch, 16, BK, true) ==
-               MPC_OK &&
-           mpc_encode_map_2d(&maps[nblk + L], base, bg.ncol, bg.nrow, 8ull * bg.pitch, 16, BM,
-                             true) == MPC_OK;
+      ok = mpc_encode_map_grouped(&maps[L], base, bg.ncol, bg.nrow, 8ull * bg.pitch, BK,
+                                  BM / 16) == MPC_OK &&
+           mpc_encode_map_grouped(&maps[kTmaMaxBlocks + L], base, bg.ncol, bg.nrow,
+                                  8ull * bg.pitch, BM, BK / 16) == MPC_OK;
     }
-    for (int i = 0; ok && i < 2; ++i)
-      ok = mpc_encode_map_2d(&maps[2 * nblk + i], b->Y[i], 2ull * ldc, g.ntot, 16ull * ldc, 16,
-                             BK, true) == MPC_OK;
-    if (ok) {
-      if ((rc = balloc(b, reinterpret_cast<char**>(&b->d_maps), sizeof(CUtensorMap) * maps.size())))
-        return rc;
-      CK(cudaMemcpy(b->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(),
-                    cudaMemcpyHostToDevice));
-    }
+    // the product buffers, once per column tile width of the TMA shapes
+    for (int sh = 0; ok && sh < kNumTmaShapes; ++sh)
+      for (int i = 0; ok && i < 2; ++i)
+        ok = mpc_encode_map_grouped(&b->ymaps[sh][i], b->Y[i], 2ull * ldc, g.ntot, 16ull * ldc,
+                                    BK, kTmaShapes[sh].bn / 16) == MPC_OK;
     b->tma_ok = ok;
   }
   CK(cudaMemsetAsync(b->X, 0, nel * sizeof(double2), c->stream));
@@ -531,7 +529,9 @@ int launch_horner_tma(mpc_ctx* c, int p, int ncol, int shape) {
   mpc_batch_state* b = c->batch;
   HornerTmaArgs h{};
   h.a = stage_args(c, p, ncol, 1.0, 1.0, false);
-  h.maps = b->d_maps;
+  for (size_t i = 0; i < b->maps.size(); ++i) h.maps[i] = b->maps[i];
+  h.maps[2 * kTmaMaxBlocks] = b->ymaps[shape][0];
+  h.maps[2 * kTmaMaxBlocks + 1] = b->ymaps[shape][1];
   h.Y[0] = b->Y[0];
   h.Y[1] = b->Y[1];
   h.status = c->d_status;

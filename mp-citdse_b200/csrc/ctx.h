@@ -21,6 +21,11 @@ int mpc_internal_fail(int code, const char* msg);
 int mpc_encode_map_2d(CUtensorMap* m, const void* base, unsigned long long inner,
                       unsigned long long outer, unsigned long long row_bytes, unsigned box_inner,
                       unsigned box_outer, bool swizzle128);
+// A 3-D FP64 tensor map over [rows][cols] viewed as 16-column groups
+// (mpc_tdse.cu).
+int mpc_encode_map_grouped(CUtensorMap* m, const void* base, unsigned long long cols,
+                           unsigned long long rows, unsigned long long row_bytes,
+                           unsigned box_rows, unsigned box_groups);
 
 #define CK(call)                                                                         \
   do {                                                                                   \

@@ -94,6 +94,27 @@ int mpc_encode_map_2d(CUtensorMap* m, const void* base, unsigned long long inner
   return MPC_OK;
 }
 
+// A 3-D FP64 tensor map over a row-major [rows][cols] matrix (rows
+// row_bytes apart) viewed as [cols / 16 groups][rows][16]: boxes of
+// {16, box_rows, box_groups} with the 128-byte swizzle.  Columns past cols
+// in the last group read the row padding (the caller keeps it zero).
+int mpc_encode_map_grouped(CUtensorMap* m, const void* base, unsigned long long cols,
+                           unsigned long long rows, unsigned long long row_bytes,
+                           unsigned box_rows, unsigned box_groups) {
+  EncodeTiledFn enc = nullptr;
+  int rc;
+  if ((rc = get_encode(&enc))) return rc;
+  cuuint64_t dims[3] = {16, (cuuint64_t)rows, (cuuint64_t)((cols + 15) / 16)};
+  cuuint64_t strides[2] = {(cuuint64_t)row_bytes, 128};
+  cuuint32_t box[3] = {16, (cuuint32_t)box_rows, (cuuint32_t)box_groups};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(base), dims, strides,
+                   box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(MPC_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return MPC_OK;
+}
+
 namespace {
 
 template <class T>

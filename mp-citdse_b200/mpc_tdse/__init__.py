@@ -298,8 +298,10 @@ class Context:
         return [(int(a), int(b), int(c), int(d), float(e)) for a, b, c, d, e in tab[:r]]
 
     def batch_fixed_plan(self):
-        """Rows of (pulses, persistent, tile width, ring depth, us per step)
-        chosen for the batched fixed step."""
+        """Rows of (pulses, kind, tile width, ring depth, us per step) chosen
+        for the batched fixed step; kind 0: one cp.async-fed launch per
+        Horner product, 1: one persistent launch, 2: one TMA-fed launch per
+        product."""
         cap = 32
         tab = np.zeros((cap, 5))
         r = lib().mpc_batch_fixed_plan(self._h, _ptr(tab), cap)

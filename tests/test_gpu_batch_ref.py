@@ -208,7 +208,7 @@ def test_persistent_step_equals_one_launch_per_product(monkeypatch):
     assert np.array_equal(n1, n2, equal_nan=True)
 
 
-@pytest.mark.parametrize("shape", [1, 2])
+@pytest.mark.parametrize("shape", [1, 2, 3, 4])
 @pytest.mark.parametrize("system", ["uneven_v", "h1e"])
 def test_tma_step_equals_cp_async_step(monkeypatch, shape, system):
     """The TMA-fed product launches (swizzled tiles read through permuted
