@@ -522,7 +522,28 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const ProdSel& ps
       for (int mt = 0; mt < WM_TILES; ++mt) nsum[mt] = 0.0;
       const double F = qv ? a.Fs[q] : 0.0;
       const double hq = qv ? a.h[q] : 0.0;
+      const double nq = (qv && ps.stage == 0) ? a.nrm[q] : 1.0;
       const double vs = ps.vscale, gm = ps.hg;
+      // every operand of the thread's elements first, so that their loads are
+      // in flight together (the stores below may alias them as far as the
+      // compiler knows, which would otherwise order each element's loads
+      // after the previous element's stores)
+      double2 yv[WM_TILES][2], xv[WM_TILES][2];
+      double ev[WM_TILES][2];
+#pragma unroll
+      for (int mt = 0; mt < WM_TILES; ++mt)
+#pragma unroll
+        for (int hr = 0; hr < 2; ++hr) {
+          const int r = r0 + wm * (WMT * 16) + mt * 16 + gq + 8 * hr;
+          yv[mt][hr] = xv[mt][hr] = make_double2(0.0, 0.0);
+          ev[mt][hr] = 0.0;
+          if (!qv || r >= nL) continue;
+          const long long i = g.state_off[L] + r;
+          const long long idx = i * a.ldc + q;
+          yv[mt][hr] = ps.Yin[idx];
+          if (ps.stage != 0) xv[mt][hr] = a.X[idx];
+          ev[mt][hr] = a.eps[i];
+        }
 #pragma unroll
       for (int mt = 0; mt < WM_TILES; ++mt)
 #pragma unroll
@@ -536,8 +557,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const ProdSel& ps
           if (ps.stage == 0) {
             // x = x_new / ||x_new|| (the reference's c /= ||c||), its coupling
             // D x = (D x_new) / ||x_new||
-            const double nq = a.nrm[q];
-            const double2 z = ps.Yin[idx];
+            const double2 z = yv[mt][hr];
             x = make_double2(z.x / nq, z.y / nq);
             a.Xw[idx] = x;
             wre = vs * (acc[mt][nt][2 * hr] / nq);
@@ -546,11 +566,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const ProdSel& ps
           } else {
             wre = vs * acc[mt][nt][2 * hr];
             wim = vs * acc[mt][nt][2 * hr + 1];
-            const double2 v0 = ps.Yin[idx];
+            const double2 v0 = yv[mt][hr];
             v = make_double2(vs * v0.x, vs * v0.y);
-            x = a.X[idx];
+            x = xv[mt][hr];
           }
-          const double e = a.eps[i];
+          const double e = ev[mt][hr];
           double kre, kim;  // M(F) v, formed as the stage form forms k
           if (a.gauge == 0) {
             kre = fma(F, wim, e * v.y);

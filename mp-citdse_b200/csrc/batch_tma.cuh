@@ -461,7 +461,25 @@ __global__ void __launch_bounds__(BTHREADS, (tma_two_per_sm<BN, NS>() ? 2 : 1))
     const bool qv = q < a.ncol;
     const double F = qv ? a.Fs[q] : 0.0;
     const double hq = qv ? a.h[q] : 0.0;
+    const double nq = (qv && ps.stage == 0) ? a.nrm[q] : 1.0;
     const double vs = ps.vscale, gm = ps.hg;
+    // operands of the thread's elements first: their loads in flight together
+    double2 yv[WMT][2], xv[WMT][2];
+    double ev[WMT][2];
+#pragma unroll
+    for (int mt = 0; mt < WMT; ++mt)
+#pragma unroll
+      for (int hr = 0; hr < 2; ++hr) {
+        const int r = r0 + 16 * (wm * WMT + mt) + frag_row(gq + 8 * hr);
+        yv[mt][hr] = xv[mt][hr] = make_double2(0.0, 0.0);
+        ev[mt][hr] = 0.0;
+        if (!qv || r >= nL) continue;
+        const long long i = g.state_off[L] + r;
+        const long long idx = i * a.ldc + q;
+        yv[mt][hr] = ps.Yin[idx];
+        if (ps.stage != 0) xv[mt][hr] = a.X[idx];
+        ev[mt][hr] = a.eps[i];
+      }
 #pragma unroll
     for (int mt = 0; mt < WMT; ++mt)
 #pragma unroll
@@ -478,8 +496,7 @@ __global__ void __launch_bounds__(BTHREADS, (tma_two_per_sm<BN, NS>() ? 2 : 1))
           double2 v, x;
           if (ps.stage == 0) {
             // x = x_new / ||x_new||, D x = (D x_new) / ||x_new||
-            const double nq = a.nrm[q];
-            const double2 z = ps.Yin[idx];
+            const double2 z = yv[mt][hr];
             x = make_double2(z.x / nq, z.y / nq);
             a.Xw[idx] = x;
             wre = vs * (accr / nq);
@@ -488,11 +505,11 @@ __global__ void __launch_bounds__(BTHREADS, (tma_two_per_sm<BN, NS>() ? 2 : 1))
           } else {
             wre = vs * accr;
             wim = vs * acci;
-            const double2 v0 = ps.Yin[idx];
+            const double2 v0 = yv[mt][hr];
             v = make_double2(vs * v0.x, vs * v0.y);
-            x = a.X[idx];
+            x = xv[mt][hr];
           }
-          const double e = a.eps[i];
+          const double e = ev[mt][hr];
           double kre, kim;
           if (a.gauge == 0) {
             kre = fma(F, wim, e * v.y);
