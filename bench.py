@@ -384,7 +384,8 @@ def measure_batched_ref(local, stream_cls, rank=0, world=1, dist=None, dt=0.05):
         "tiles": [{"pulses": a, "tile_cols": b, "stages": c, "k_split": d, "us_per_rhs": e}
                   for a, b, c, d, e in tiles],
         "step_plan": [{"pulses": a,
-                       "launch": ("per-product", "persistent", "per-product-tma")[b],
+                       "launch": ("per-product", "persistent", "per-product-tma",
+                                  "per-product-split")[b],
                        "tile_cols": c, "ring": d, "us_per_step": e}
                       for a, b, c, d, e in plan],
         "roofline": {"bound": "tensor", "achieved": live_tflops, "peak": dmma, "unit": "TFLOP/s",

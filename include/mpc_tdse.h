@@ -229,13 +229,15 @@ int mpc_batch_autotune(mpc_ctx *ctx, int B, double *table, int cap);
 
 /* How the batched fixed step (mpc_batch_advance) ran at each width: on its
  * first use the library times, at widths 1, 2, 4, ... pulses, a whole step
- * as one launch per Horner product (cp.async-fed tiles), as one persistent
- * launch on each unsplit tile shape, and as one TMA-fed launch per product
- * on each TMA tile shape, and keeps the fastest (every choice gives the same
- * bits).  Rows of 5 doubles, up to cap: pulses, kind (0 one cp.async-fed
- * launch per product, 1 persistent, 2 one TMA-fed launch per product), tile
- * width (real columns), ring depth, microseconds per step.  Returns the
- * number of rows (0 before any fixed-step call). */
+ * as one launch per Horner product on each cp.async-fed tile variant, as one
+ * persistent launch on each unsplit tile shape, and as one TMA-fed launch per
+ * product on each TMA tile shape, and keeps the fastest (every choice gives
+ * the same bits).  Rows of 5 doubles, up to cap: pulses, kind (0 one
+ * cp.async-fed launch per product, 1 persistent, 2 one TMA-fed launch per
+ * product, 3 one cp.async-fed launch per product with each tile's two
+ * coupled blocks in two CTAs), tile width (real columns), ring depth,
+ * microseconds per step.  Returns the number of rows (0 before any
+ * fixed-step call). */
 int mpc_batch_fixed_plan(mpc_ctx *ctx, double *table, int cap);
 
 /* Objective and gradient (new: the reference has no gradients).

@@ -328,7 +328,8 @@ struct mpc_batch_state {
   std::vector<int> tile;
   std::vector<double> tile_us;
   // fixed-step steps, per width bucket: -1 one launch per Horner product
-  // (with the tuned variant), v >= 0 the persistent launch on variant v,
+  // (on the right-hand-side tuner's variant), kPlanPerProduct + v one launch
+  // per product on variant v, v >= 0 the persistent launch on variant v,
   // kPlanTma + s one TMA-fed launch per product on TMA shape s;
   // microseconds per step of the choice
   std::vector<int> hplan;
@@ -341,6 +342,7 @@ struct mpc_batch_state {
 
 namespace {
 constexpr int kPlanTma = 100;
+constexpr int kPlanPerProduct = 200;
 }
 
 namespace {
@@ -474,6 +476,8 @@ int horner_plan(mpc_ctx* c, int ncol) {
   const mpc_batch_state* b = c->batch;
   if (c->force_tma > 0 && b->tma_ok) return kPlanTma + std::min(c->force_tma - 1, kNumTmaShapes - 1);
   if (c->force_persist) return mpc_batch_variant(c, ncol);
+  if (c->forced_variant >= 0 && c->forced_variant < kNumVariants)
+    return kPlanPerProduct + c->forced_variant;
   const int j = width_bucket(ncol);
   if (j < (int)b->hplan.size()) return b->hplan[j];
   const int v = mpc_batch_variant(c, ncol);
@@ -512,7 +516,7 @@ int launch_horner_persistent_v(mpc_ctx* c, int ncol, int v) {
 // v_m = h M(F) v_{m+1} + G[m] x for m = 11 .. 0, and v_0 = x_new.  Product p
 // forms v_{11-p}; the same ping-pong buffers as the stage form, so x_new
 // lands in Y[0].
-int launch_horner(mpc_ctx* c, int p, int ncol) {
+int launch_horner(mpc_ctx* c, int p, int ncol, int v = -1) {
   StageArgs a = stage_args(c, p, ncol, 1.0, 1.0, false);
   if (p == 0) a.Yin = c->batch->Y[0];   // the previous step's unnormalised x_new
   a.hg = rkf78::G[11 - p];
@@ -520,7 +524,7 @@ int launch_horner(mpc_ctx* c, int p, int ncol) {
   a.hlast = (p == 11) ? 1 : 0;
   ProfScope ps(c, MPC_KERNEL_BATCH_STAGE);
   ++c->launches;
-  CK(launch_variant<2>(c->stream, mpc_batch_variant(c, a.ncol), a));
+  CK(launch_variant<2>(c->stream, v >= 0 ? v : mpc_batch_variant(c, a.ncol), a));
   return MPC_OK;
 }
 
@@ -548,6 +552,11 @@ int launch_horner_tma(mpc_ctx* c, int p, int ncol, int shape) {
 // The 12 products of one fixed step of ncol pulses, run as plan says.
 int launch_horner_plan(mpc_ctx* c, int ncol, int plan) {
   int rc;
+  if (plan >= kPlanPerProduct) {
+    for (int p = 0; p < 12; ++p)
+      if ((rc = launch_horner(c, p, ncol, plan - kPlanPerProduct))) return rc;
+    return MPC_OK;
+  }
   if (plan >= kPlanTma) {
     for (int p = 0; p < 12; ++p)
       if ((rc = launch_horner_tma(c, p, ncol, plan - kPlanTma))) return rc;
@@ -630,7 +639,11 @@ int autotune_horner(mpc_ctx* c, int max_cols) {
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  std::vector<int> cands = {-1, 0, 1, 2, 3, 4};
+  // one launch per product on every tile variant (the right-hand-side
+  // tuner's choice need not suit the Horner epilogue), the persistent launch
+  // on every unsplit variant, the TMA-fed launches
+  std::vector<int> cands = {0, 1, 2, 3, 4};
+  for (int v = 0; v < kNumVariants; ++v) cands.push_back(kPlanPerProduct + v);
   if (b->tma_ok && !c->no_tma)
     for (int sh = 0; sh < kNumTmaShapes; ++sh) cands.push_back(kPlanTma + sh);
   int rc = MPC_OK;
@@ -734,7 +747,12 @@ int mpc_batch_fixed_plan(mpc_ctx* c, double* table, int cap) {
   for (int j = 0; table && j < rows && j < cap; ++j) {
     const int v = b->hplan[j];
     table[5 * j + 0] = std::min(1 << j, b->ldc);
-    if (v >= kPlanTma) {
+    if (v >= kPlanPerProduct) {
+      const TileVariant& tv = kVariants[v - kPlanPerProduct];
+      table[5 * j + 1] = tv.split ? 3 : 0;
+      table[5 * j + 2] = tv.bn;
+      table[5 * j + 3] = tv.nst;
+    } else if (v >= kPlanTma) {
       table[5 * j + 1] = 2;
       table[5 * j + 2] = kTmaShapes[v - kPlanTma].bn;
       table[5 * j + 3] = kTmaShapes[v - kPlanTma].ns;

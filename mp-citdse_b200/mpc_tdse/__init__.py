@@ -301,7 +301,7 @@ class Context:
         """Rows of (pulses, kind, tile width, ring depth, us per step) chosen
         for the batched fixed step; kind 0: one cp.async-fed launch per
         Horner product, 1: one persistent launch, 2: one TMA-fed launch per
-        product."""
+        product, 3: as 0 with each tile's coupled blocks in two CTAs."""
         cap = 32
         tab = np.zeros((cap, 5))
         r = lib().mpc_batch_fixed_plan(self._h, _ptr(tab), cap)

@@ -170,8 +170,9 @@ def test_autotune_table_and_variants_bit_identical(monkeypatch):
 def test_every_tile_variant_gives_the_same_bits(monkeypatch):
     """MPC_BATCH_VARIANT pins one of the nine stage-GEMM variants (column
     tile 16/32/64 x pipeline depth, with or without the P/Q halves in two
-    CTAs): the batched forward and the batched adjoint must not change by a
-    bit, on a 2e system whose blocks have different sizes and row-tile tails."""
+    CTAs): the batched forward, the batched adjoint and the fixed step's
+    Horner products must not change by a bit, on a 2e system whose blocks have
+    different sizes and row-tile tails."""
     from mpc_tdse.systems import helium_like_2e
 
     s = helium_like_2e((70, 90, 100), gauge="v", seed=4)
@@ -194,10 +195,13 @@ def test_every_tile_variant_gives_the_same_bits(monkeypatch):
                                                  rtol=1e-10, atol=1e-10)
             J, G, Fb = ctx.batch_objective_gradient(pulses, U, T, 0.0, 0.1, 60, X0, -1,
                                                     ckpt_every=16)
-        out.append((X, acc, rej, J, G, Fb))
+            # the fixed step's Horner products, one launch each on variant v
+            Xf, pf, nf = ctx.batch_advance(pulses, 0.0, 0.05, [30 + 3 * b for b in range(11)],
+                                           X0, history=True)
+        out.append((X, acc, rej, J, G, Fb, Xf, pf, nf))
     for v in range(1, 9):
         for a, b in zip(out[0], out[v]):
-            assert np.array_equal(a, b), v
+            assert np.array_equal(a, b, equal_nan=True), v
 
 
 def test_single_pulse_adaptive_and_batch_names():
