@@ -16,6 +16,10 @@
 //   for the last stage x_new = x + sum_j (dt*b_j) k_j with a per-CTA partial of
 //   ||x_new||^2.  Products and sums are rounded separately (no contraction),
 //   left to right, as the CPU restatement does.
+//   Horner form (a.horner; the frozen-field step as the method's stability
+//   polynomial R(z) = sum_m G_m z^m, degree 12): the input is v_{m+1} scaled
+//   by vscale (G_12 for the first product, else 1) and the output
+//   v_m = dt * M(F) (vscale v_{m+1}) + G_m x, v_0 = x_new; k is not stored.
 // k_renorm: ||x_new|| from the per-CTA partials in a fixed order, then
 //   x = x_new / ||x_new|| element by element (c /= ||c||, src/tdse/tdse.cpp:
 //   194-198) and the tracked population |x[pop]|^2 (:200-204).
@@ -42,6 +46,8 @@ struct CombineArgs {
   int ncoef;               // non-zero weights of the next combination
   int coef_j[kNumStages];
   double coef[kNumStages]; // dt * a_{s+1,j}  (or dt * b_j)
+  int horner;              // 1: one Horner product (stage 12: the last, with norm partials)
+  double vscale, hg, hstep;
   Geometry g;
 };
 
@@ -95,7 +101,29 @@ __global__ void __launch_bounds__(kCombineThreads)
     P.y = dadd(P.y, __shfl_xor_sync(0xffffffffu, P.y, o));
   }
   double nsq = 0.0;
-  if (valid && q == 0) {
+  if (valid && q == 0 && a.horner) {
+    const double F = a.Ftab[a.step];
+    const double e = a.eps[i];
+    const double vs = a.vscale;
+    const double2 yr = a.y[i];
+    const double2 xi = a.x[i];
+    const double2 y = make_double2(dmul(vs, yr.x), dmul(vs, yr.y));
+    P = make_double2(dmul(vs, P.x), dmul(vs, P.y));
+    Q = make_double2(dmul(vs, Q.x), dmul(vs, Q.y));
+    double kre = dmul(e, y.y);
+    double kim = dmul(-e, y.x);
+    if (a.gauge == 0) {
+      if (L > 0) { kim = dadd(kim, dmul(-F, P.x)); kre = dadd(kre, dmul(F, P.y)); }
+      if (L < g.nblk) { kim = dadd(kim, dmul(-F, Q.x)); kre = dadd(kre, dmul(F, Q.y)); }
+    } else {
+      if (L > 0) { kre = dadd(kre, dmul(F, P.x)); kim = dadd(kim, dmul(F, P.y)); }
+      if (L < g.nblk) { kre = dadd(kre, dmul(-F, Q.x)); kim = dadd(kim, dmul(-F, Q.y)); }
+    }
+    const double2 o = make_double2(dadd(dmul(a.hstep, kre), dmul(a.hg, xi.x)),
+                                   dadd(dmul(a.hstep, kim), dmul(a.hg, xi.y)));
+    a.out[i] = o;
+    nsq = dadd(dmul(o.x, o.x), dmul(o.y, o.y));
+  } else if (valid && q == 0) {
     const double F = a.Ftab[a.step];
     const double e = a.eps[i];
     const double2 y = a.y[i];

@@ -52,6 +52,7 @@ struct mpc_ctx {
   double* d_D = nullptr;
   double2* d_x = nullptr;
   double2* d_y = nullptr;
+  double2* d_v = nullptr;   // Horner products' second buffer (zero tail like d_x, d_y)
   double2* d_k = nullptr;
   double2* d_RP = nullptr;
   double2* d_CP = nullptr;
@@ -97,6 +98,9 @@ struct mpc_ctx {
   // MPC_NO_TMA=1: the fixed-step tuner leaves the TMA-fed launches out
   int force_tma = 0;
   bool no_tma = false;
+  // MPC_STAGE_FORM=1 at context creation: the streamed single-pulse steps as
+  // 13 stages instead of the 12 Horner products of the stability polynomial
+  bool stage_form = false;
   // grid-barrier wait limit of the persistent kernels (mpc_ctx_set_wait_limit)
   unsigned long long wait_limit_ns = 2000000000ull;
   // the next persistent launch gets an unreachable barrier target

@@ -356,6 +356,44 @@ int rk78_step_dev(mpc_ctx* c, int step, double dt) {
   return MPC_OK;
 }
 
+// One fixed step of the state in d_x with field Ftab[step] as the 12 Horner
+// products of the RKF78 stability polynomial (the same step: with the field
+// frozen the system is linear and autonomous, and R(hM)x is what the 13
+// stages form), each a dipole stream and a combine pass: one stream pass per
+// step fewer than the stage form.  Result in d_y (not renormalised).
+int horner_step_dev(mpc_ctx* c, int step, double dt) {
+  int rc;
+  for (int p = 0; p < 12; ++p) {
+    // d_x -> d_v -> d_y -> d_v -> ... -> d_y (p = 11)
+    const double2* in = (p == 0) ? c->d_x : ((p - 1) % 2 == 1 ? c->d_y : c->d_v);
+    double2* out = (p % 2 == 1) ? c->d_y : c->d_v;
+    if ((rc = launch_stream(c, in))) return rc;
+    CombineArgs a{};
+    a.x = c->d_x;
+    a.y = in;
+    a.k = c->d_k;
+    a.out = out;
+    a.eps = c->d_eps;
+    a.RP = c->d_RP;
+    a.CP = c->d_CP;
+    a.strip_slot0 = c->d_strip_slot0;
+    a.Ftab = c->d_Ftab;
+    a.norm_part = c->d_norm_part;
+    a.step = step;
+    a.stage = (p == 11) ? kNumStages - 1 : 0;   // the last product forms the norm partials
+    a.gauge = (c->gauge == 'l') ? 0 : 1;
+    a.horner = 1;
+    a.vscale = (p == 0) ? rkf78::G[12] : 1.0;
+    a.hg = rkf78::G[11 - p];
+    a.hstep = dt;
+    a.g = c->g;
+    ProfScope ps(c, MPC_KERNEL_COMBINE);
+    CK(mpc_launch_pdl(k_stage_combine, dim3(c->combine_grid), dim3(kCombineThreads), 0,
+                      c->stream, a));
+  }
+  return MPC_OK;
+}
+
 __global__ void k_pop_init(const double2* x, int pop_index, double* pop) {
   const double2 v = x[pop_index];
   pop[0] = __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y));
@@ -436,7 +474,7 @@ int run_steps(mpc_ctx* c, double dt, int steps, int pop_index) {
   k_pop_init<<<1, 1, 0, c->stream>>>(c->d_x, pop_index, c->d_pop);
   CK(cudaGetLastError());
   for (int st = 0; st < steps; ++st) {
-    if ((rc = rk78_step_dev(c, st, dt))) return rc;
+    if ((rc = c->stage_form ? rk78_step_dev(c, st, dt) : horner_step_dev(c, st, dt))) return rc;
     if ((rc = launch_renorm(c, st, pop_index))) return rc;
   }
   return MPC_OK;
@@ -543,6 +581,7 @@ int mpc_ctx_create(int L_max, const int* state_sz, const double* eig, const doub
   c->force_persist = std::getenv("MPC_FORCE_PERSIST") != nullptr;
   if (const char* ft = std::getenv("MPC_FORCE_TMA")) c->force_tma = std::max(0, std::atoi(ft));
   c->no_tma = std::getenv("MPC_NO_TMA") != nullptr;
+  c->stage_form = std::getenv("MPC_STAGE_FORM") != nullptr;
   c->gauge = gauge;
   c->n.assign(state_sz, state_sz + L_max + 1);
   CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
@@ -565,6 +604,7 @@ int mpc_ctx_create(int L_max, const int* state_sz, const double* eig, const doub
     return bail(fail(MPC_ERR_CUDA, "cudaStreamCreate failed"));
   if ((rc = dalloc(c, &c->d_eps, g.ntot)) || (rc = dalloc(c, &c->d_D, d_total)) ||
       (rc = dalloc(c, &c->d_x, g.ntot + kVecPad)) || (rc = dalloc(c, &c->d_y, g.ntot + kVecPad)) ||
+      (rc = dalloc(c, &c->d_v, g.ntot + kVecPad)) ||
       (rc = dalloc(c, &c->d_k, (size_t)kNumStages * g.ntot)) ||
       (rc = dalloc(c, &c->d_RP, rp_total)) ||
       (rc = dalloc(c, &c->d_CP, (size_t)nslots * kStripW)) ||
@@ -582,6 +622,7 @@ int mpc_ctx_create(int L_max, const int* state_sz, const double* eig, const doub
       cudaMemset(c->d_status, 0, sizeof(unsigned)) != cudaSuccess ||
       cudaMemset(c->d_x, 0, sizeof(double2) * (g.ntot + kVecPad)) != cudaSuccess ||
       cudaMemset(c->d_y, 0, sizeof(double2) * (g.ntot + kVecPad)) != cudaSuccess ||
+      cudaMemset(c->d_v, 0, sizeof(double2) * (g.ntot + kVecPad)) != cudaSuccess ||
       cudaMemset(c->d_D, 0, sizeof(double) * d_total) != cudaSuccess)
     return bail(fail(MPC_ERR_CUDA, "upload failed"));
   const double* src = dip;
