@@ -224,3 +224,28 @@ def test_full_size_2e_short_propagation_matches_oracle(oracle, he2e):
         oracle.use_plain_loops()
     assert np.max(np.abs(np.abs(ct) ** 2 - np.abs(cto) ** 2)) < 1e-12
     assert np.max(np.abs(nrm - nrmo)) < 1e-12
+
+
+@pytest.mark.parametrize("gauge", ["l", "v"])
+def test_horner_steps_equal_stage_form(monkeypatch, gauge):
+    """The streamed path's fixed step as the 12 Horner products of the RKF78
+    stability polynomial against the same step as 13 stages (MPC_STAGE_FORM):
+    the same frozen-field step, so the same state up to rounding, over a
+    whole short pulse; both against the oracle."""
+    s = _sys("multistrip", gauge, seed=7)
+    x0 = _x(s.ntot, seed=8)
+    Io, w = mpc_tdse.to_au(2e14, 1.5498)
+    p = mpc_tdse.pulse_setup("sine", gauge, Io, w, 0.0, 2, 0.0)
+    out = []
+    for stage_form in (False, True):
+        if stage_form:
+            monkeypatch.setenv("MPC_STAGE_FORM", "1")
+        with mpc_tdse.Context.from_system(s) as ctx:
+            ctx.set_path("streaming")
+            out.append(ctx.propagate(p, 0.0, 0.1, 120, x0))
+    (ct_h, pop_h, fld_h, nrm_h), (ct_s, pop_s, fld_s, nrm_s) = out
+    assert np.array_equal(fld_h, fld_s)
+    assert np.max(np.abs(ct_h - ct_s)) < 1e-12
+    assert np.max(np.abs(pop_h - pop_s)) < 1e-12
+    assert np.max(np.abs(nrm_h - nrm_s)) < 1e-12
+    assert not np.array_equal(ct_h, ct_s)   # the two forms did run
