@@ -449,6 +449,9 @@ def batched_kernel_case(local):
 
     os.environ["MPC_NO_AUTOTUNE"] = "1"
     os.environ["MPC_BATCH_VARIANT"] = "2"
+    # the persistent launch unless MPC_NO_PERSIST (one launch per product on
+    # the pinned variant) or MPC_FORCE_TMA (the TMA-fed launches) asks otherwise
+    os.environ.setdefault("MPC_FORCE_PERSIST", "1")
     import mpc_tdse
     from mpc_tdse.structure1e import hydrogen
 
