@@ -139,6 +139,14 @@ __device__ __forceinline__ void bulk_load(void* smem_dst, const void* src, uint3
       : "memory");
 }
 
+// An L2 policy that marks lines to be kept over normal and evict-first ones:
+// for the part of the dipole blocks that stays in L2 from one pass to the next.
+__device__ __forceinline__ uint64_t make_evict_last_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
 // An L2 policy that marks lines for early eviction: for data streamed once
 // per pass (the dipole blocks), so that the small, reused vectors stay.
 __device__ __forceinline__ uint64_t make_evict_first_policy() {

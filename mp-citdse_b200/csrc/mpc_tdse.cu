@@ -660,6 +660,18 @@ int mpc_ctx_create(int L_max, const int* state_sz, const double* eig, const doub
   c->sargs.cta_slot0 = c->d_cta_slot0;
   c->sargs.status = c->d_status;
   c->sargs.g = c->g;
+  {
+    // dipole bytes kept in L2 across the passes of a step (MPC_L2_KEEP_MB
+    // overrides): the rest streams through with an evict-first hint.  40 MB
+    // of the 126 MB L2: on the 547 MB He CI couplings 0 / 24 / 32 / 40 / 48 /
+    // 64 / 128 MB gave 856-868 / 869 / 872-893 / 876 / 876 / 883 / 863
+    // pulse-steps/s (two boxes)
+    double keep_mb = 40.0;
+    if (const char* e = std::getenv("MPC_L2_KEEP_MB")) keep_mb = std::atof(e);
+    const double dbytes = 8.0 * (double)d_total;
+    c->sargs.keep_frac =
+        dbytes > 0.0 ? (float)std::min(1.0, std::max(0.0, keep_mb * 1048576.0 / dbytes)) : 0.0f;
+  }
   if ((rc = ensure_hist(c, 1024))) return bail(rc);
   *out = c;
   return MPC_OK;

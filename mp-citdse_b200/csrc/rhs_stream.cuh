@@ -78,7 +78,9 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
       pdl_wait();
       return;
     }
-    const uint64_t policy = make_evict_first_policy();
+    const uint64_t stream_policy = make_evict_first_policy();
+    const uint64_t keep_policy = make_evict_last_policy();
+    const int keep_end = t_begin + (int)(a.keep_frac * (float)(t_end - t_begin));
     // The dipole blocks do not change between launches: the first ring's
     // worth of tiles is requested before waiting for the previous kernel;
     // their stage-vector rows (written by that kernel) only after it.
@@ -88,7 +90,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
       decode_tile(g, t_begin + i, b, s, rt);
       mbar_arrive_expect_tx(&full[i], kTileBytes + kYRowBytes);
       tma_load_2d_hint(tiles + i * (kTileR * kStripW), &tm.m[b], &full[i], s * kStripW,
-                       rt * kTileR, policy);
+                       rt * kTileR, t_begin + i < keep_end ? keep_policy : stream_policy);
     }
     pdl_wait();
     int issued = 0;
@@ -101,7 +103,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
         if (!mbar_wait_bounded(&empty[stage], (round - 1) & 1, a.status)) break;
         mbar_arrive_expect_tx(&full[stage], kTileBytes + kYRowBytes);
         tma_load_2d_hint(tiles + stage * (kTileR * kStripW), &tm.m[b], &full[stage],
-                         s * kStripW, rt * kTileR, policy);
+                         s * kStripW, rt * kTileR, t < keep_end ? keep_policy : stream_policy);
       }
       // the tile's 16 rows of the stage vector (the vector carries a zeroed
       // tail of kVecPad entries, so the last tile never reads past it)

@@ -18,6 +18,9 @@ struct StreamArgs {
   double2* CP;            // column partial slots, kStripW complex each
   const int* cta_slot0;   // first CP slot of each CTA
   unsigned* status;
+  // the first keep_frac of every CTA's tiles are loaded with an L2 evict-last
+  // hint (they stay in L2 from pass to pass), the rest evict-first
+  float keep_frac;
   Geometry g;
 };
 
