@@ -249,3 +249,20 @@ def test_horner_steps_equal_stage_form(monkeypatch, gauge):
     assert np.max(np.abs(pop_h - pop_s)) < 1e-12
     assert np.max(np.abs(nrm_h - nrm_s)) < 1e-12
     assert not np.array_equal(ct_h, ct_s)   # the two forms did run
+
+
+def test_l2_keep_hint_changes_no_bit(monkeypatch):
+    """The dipole stream's L2 evict-last share (MPC_L2_KEEP_MB) is a cache
+    hint only: the same bits with none of the couplings kept and with all."""
+    s = _sys("multistrip", "l", seed=9)
+    x0 = _x(s.ntot, seed=10)
+    Io, w = mpc_tdse.to_au(1e14, 1.5498)
+    p = mpc_tdse.pulse_setup("sine", "l", Io, w, 0.0, 2, 0.0)
+    out = []
+    for keep in ("0", "100000"):
+        monkeypatch.setenv("MPC_L2_KEEP_MB", keep)
+        with mpc_tdse.Context.from_system(s) as ctx:
+            ctx.set_path("streaming")
+            out.append(ctx.propagate(p, 0.0, 0.1, 40, x0))
+    for u, v in zip(*out):
+        assert np.array_equal(u, v)
