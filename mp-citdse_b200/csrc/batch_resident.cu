@@ -14,6 +14,9 @@
 // every row held in registers), writes k_s and the next stage input, and
 // meets the other CTAs at a grid barrier: 13 barriers per attempted step.
 //
+// In fixed-step mode (the reference's semantics) an attempt is the frozen-
+// field step as the 12 Horner products of its stability polynomial, one
+// barrier each, instead of the 13 stages.
 // Step control needs no extra barrier: after the last stage every CTA
 // reduces the per-CTA norm and error partials in the same fixed order and
 // makes the same accept / reject decision for every pulse (the decision
@@ -46,6 +49,7 @@ constexpr int kMaxP = 8;         // widest launch (pulse columns)
 
 __constant__ double q_A[13][13];
 __constant__ double q_B8[13];
+__constant__ double q_G[13];     // the stability polynomial's coefficients
 __constant__ double q_E[13];     // b8 - b7
 __constant__ double q_C[13];
 
@@ -235,7 +239,11 @@ __global__ void __launch_bounds__(QT, 1) k_batch_res(const __grid_constant__ BrA
     }
     __syncthreads();
 
-    for (int s = 0; s < kNumStages; ++s) {
+    // fixed-step mode: the frozen-field step as the 12 Horner products of its
+    // stability polynomial (v_12 = G_12 x, v_m = h M(F) v_{m+1} + G_m x,
+    // x_new = v_0), one grid barrier each; otherwise the 13 stages
+    const int nst = a.fx.on ? 12 : kNumStages;
+    for (int s = 0; s < nst; ++s) {
       // ---- stage input: the coupled blocks' rows and this CTA's own rows ----
       if (s == 0) {
         for (int e = tid; e < Kc * P; e += QT) {
@@ -270,7 +278,7 @@ __global__ void __launch_bounds__(QT, 1) k_batch_res(const __grid_constant__ BrA
         }
       }
       __syncthreads();
-      const bool last_stage = (s == kNumStages - 1);
+      const bool last_stage = (s == nst - 1);
       double2* Yout = ((s + 1) & 1) ? a.Y1 : a.Y0;
       // ---- coupling sums W[li][q] = sum_k crow[k][li] win[k][q], then k_s ----
       for (int rg = 0; rg < nrows; rg += kRowGroup) {
@@ -319,8 +327,14 @@ __global__ void __launch_bounds__(QT, 1) k_batch_res(const __grid_constant__ BrA
           }
           const int i = row0 + li;
           const double ev = a.eps[i];
-          const double2 y = ysm[li * P + q];
+          double2 y = ysm[li * P + q];
           const double F = s_F[s][q];
+          if (a.fx.on && s == 0) {   // v_12 = G_12 x: its coupling G_12 (D x)
+            const double vs = q_G[12];
+            y = make_double2(vs * y.x, vs * y.y);
+            wre *= vs;
+            wim *= vs;
+          }
           double kre, kim;
           if (a.gauge == 0) {
             kre = fma(F, wim, ev * y.y);
@@ -329,9 +343,21 @@ __global__ void __launch_bounds__(QT, 1) k_batch_res(const __grid_constant__ BrA
             kre = fma(F, wre, ev * y.y);
             kim = fma(F, wim, -ev * y.x);
           }
-          ksm[((size_t)s * nrows + li) * P + q] = make_double2(kre, kim);
           const double2 x = xsm[li * P + q];
           const double hq = s_hatt[q];
+          if (a.fx.on) {   // v_{11-s} = h M(F) v + G_{11-s} x
+            const double gm = q_G[11 - s];
+            const double2 o = make_double2(fma(hq, kre, gm * x.x), fma(hq, kim, gm * x.y));
+            if (!last_stage) {
+              if (q < ncol) Yout[(long long)i * ldc + q] = o;
+            } else {
+              rerr[li * P + q] = 0.0;
+              rnrm[li * P + q] = o.x * o.x + o.y * o.y;
+              if (q < ncol) a.XN[(long long)i * ldc + q] = o;
+            }
+            continue;
+          }
+          ksm[((size_t)s * nrows + li) * P + q] = make_double2(kre, kim);
           double2 o = x;
           if (!last_stage) {
 #pragma unroll
@@ -635,6 +661,7 @@ int mpc_batch_res_pmax(mpc_ctx* c) {
   }
   if (cudaMemcpyToSymbol(q_A, A, sizeof A) != cudaSuccess ||
       cudaMemcpyToSymbol(q_B8, B8, sizeof B8) != cudaSuccess ||
+      cudaMemcpyToSymbol(q_G, rkf78::G, sizeof rkf78::G) != cudaSuccess ||
       cudaMemcpyToSymbol(q_E, E, sizeof E) != cudaSuccess ||
       cudaMemcpyToSymbol(q_C, Cn, sizeof Cn) != cudaSuccess ||
       cudaMalloc(&r->part, sizeof(CtaPart) * G) != cudaSuccess ||
