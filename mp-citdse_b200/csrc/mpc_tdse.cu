@@ -790,9 +790,12 @@ int mpc_advance(mpc_ctx* c, const mpc_pulse* p, double t0, double dt, int steps,
   return run_steps(c, dt, steps, pop_index);
 }
 
-int mpc_history_get(mpc_ctx* c, int steps, double* pop_out, double* field_out,
-                    double* norm_out) {
-  if (!c) return fail(MPC_ERR_ARG, "null argument");
+}  // extern "C"
+
+namespace {
+
+// Enqueues the copies of the last run's histories (no wait).
+int history_copy(mpc_ctx* c, int steps, double* pop_out, double* field_out, double* norm_out) {
   if (steps < 0 || steps + 1 > c->hist_cap) return fail(MPC_ERR_ARG, "steps out of range");
   CK(cudaSetDevice(c->device));
   if (pop_out)
@@ -804,6 +807,18 @@ int mpc_history_get(mpc_ctx* c, int steps, double* pop_out, double* field_out,
   if (norm_out && steps > 0)
     CK(cudaMemcpyAsync(norm_out, c->d_nrm, sizeof(double) * steps, cudaMemcpyDeviceToHost,
                        c->stream));
+  return MPC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mpc_history_get(mpc_ctx* c, int steps, double* pop_out, double* field_out,
+                    double* norm_out) {
+  if (!c) return fail(MPC_ERR_ARG, "null argument");
+  int rc;
+  if ((rc = history_copy(c, steps, pop_out, field_out, norm_out))) return rc;
   return check_status(c);
 }
 
@@ -815,7 +830,8 @@ int mpc_propagate(mpc_ctx* c, const mpc_pulse* p, double t0, double dt, int step
   int rc;
   if ((rc = mpc_state_set(c, ct))) return rc;
   if ((rc = mpc_advance(c, p, t0, dt, steps, pop_index))) return rc;
-  if ((rc = mpc_history_get(c, steps, pop_out, field_out, norm_out))) return rc;
+  // the histories and the state come back behind one wait (mpc_state_get's)
+  if ((rc = history_copy(c, steps, pop_out, field_out, norm_out))) return rc;
   return mpc_state_get(c, ct);
 }
 
