@@ -269,13 +269,6 @@ __device__ __forceinline__ void tma_chunk_of(int j, int nchP, int nchQ, int& i, 
   }
 }
 
-// Product h.p of a fixed step, one tile per CTA: blockIdx.x = row tile x
-// column tiles + column tile (CTAs that read the same coupling rows run side
-// by side).  Chunk j lands in slot j % NS; the first NS are issued up front,
-// then chunk j + NS by warp j % 8 once all eight warps are done with chunk j
-// (the issuing duty rotates, so no warp carries more than an eighth of it).
-// Per chunk two TMA instructions: the coupling tile and the state tile, each
-// one 3-D box.
 // Rings small enough for two CTAs per SM (128 registers a thread) run the
 // chunks one at a time; the deeper rings (one CTA per SM, registers to
 // spare) pair them.
@@ -284,6 +277,13 @@ constexpr bool tma_two_per_sm() {
   return tma_smem<BN, NS>() <= 100 * 1024;
 }
 
+// Product h.p of a fixed step, one tile per CTA: blockIdx.x = row tile x
+// column tiles + column tile (CTAs that read the same coupling rows run side
+// by side).  Chunk j lands in slot j % NS; the first NS are issued up front,
+// then chunk j + NS by warp j % 8 once all eight warps are done with chunk j
+// (the issuing duty rotates, so no warp carries more than an eighth of it).
+// Per chunk two TMA instructions: the coupling tile and the state tile, each
+// one 3-D box.
 template <int BN, int NS>
 __global__ void __launch_bounds__(BTHREADS, (tma_two_per_sm<BN, NS>() ? 2 : 1))
     k_horner_tma(const __grid_constant__ HornerTmaArgs h) {
@@ -325,9 +325,8 @@ __global__ void __launch_bounds__(BTHREADS, (tma_two_per_sm<BN, NS>() ? 2 : 1))
   __syncthreads();
   pdl_trigger();
 
-  // chunk j into its slot (the slot's previous chunk is done): the coupling
-  // tile (coupling = false: only the state tile, the coupling tile is in
-  // flight already)
+  // chunk j into its slot (whose previous chunk is done): its coupling tile,
+  // its state tile, or both
   auto issue_part = [&](int j, bool coupling, bool state) {
     const int slot = j % NS;
     double* As = ring + slot * SLOT;
